@@ -1,0 +1,349 @@
+"""Benchmark: photon packets/s of SKIRT7's stellar-emission packet loop on the panchromatic octree
+disk galaxy (50 log-spaced wavelengths 0.1-10 micron, octree max level 10 with cell mass fraction
+< 1e-6, three 512x512 frames at 0/60/88 degrees, FP32 geometry with FP64 tallies).
+
+One step = one stellar-emission phase (one persistent launch) over all 50 wavelengths with
+--packets packets per wavelength per GPU.  Ranks (torchrun, one per GPU) run disjoint packet
+ranges of one simulation and all-reduce the frames over NCCL at the end of each step (weak
+scaling: the packets per GPU are fixed).  `value` is device-timed; `e2e` is the same metric
+through the C ABI with the tallies read back into host memory every step.
+
+--impl reference times the reference's algorithm on the host cores: the oracle (a scalar FP64
+restatement of the reference's life cycle, oracle/oracle.cpp) with all host threads on a
+bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURED = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--packets", type=float, default=1e6, help="packets per wavelength per GPU per step")
+    p.add_argument("--max-level", type=int, default=10)
+    p.add_argument("--mass-fraction", type=float, default=1e-6)
+    p.add_argument("--nlambda", type=int, default=50)
+    p.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="target duration of the CPU baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--tree-cache", default=os.path.join(ROOT, "_work", "octree_cache.npz"))
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(MEASURED) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index=0):
+        self.samples = []
+        self.index = index
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([s.strip() for s in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and "Active" in s[3 + i]
+                          and "Not" not in s[3 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def build_model(args):
+    from skirt7_b200 import models
+    return models.pan_disk(nlambda=args.nlambda, inclinations=(0, 60, 88), npix=512)
+
+
+def get_tree(args, model, device):
+    """The octree of the workload (device-sampled subdivision); cached across runs of the same size."""
+    import numpy as np
+    from skirt7_b200 import _abi as A
+    from skirt7_b200 import runtime
+    from skirt7_b200.scene import KPC, TreeDustGrid
+    ext = (-20 * KPC, -20 * KPC, -2 * KPC, 20 * KPC, 20 * KPC, 2 * KPC)
+    key = "L%d_f%g" % (args.max_level, args.mass_fraction)
+    if os.path.exists(args.tree_cache):
+        z = np.load(args.tree_cache)
+        if str(z["key"]) == key:
+            return TreeDustGrid(A.GRID_OCTREE, ext, z["box"], z["child"], z["father"], z["cell"], z["dir"],
+                                z["off"], z["ids"]), 0.0
+    t0 = time.time()
+    tree = runtime.build_tree(model, A.GRID_OCTREE, ext, minLevel=2, maxLevel=args.max_level,
+                              maxMassFraction=args.mass_fraction, sampleCount=100, seed=4357, device=device)
+    dt = time.time() - t0
+    try:
+        os.makedirs(os.path.dirname(args.tree_cache), exist_ok=True)
+        np.savez(args.tree_cache, key=key, box=tree.node_box, child=tree.node_child, father=tree.node_father,
+                 cell=tree.node_cell, dir=tree.node_dir, off=tree.nbr_offsets, ids=tree.nbr_ids)
+    except Exception:
+        pass
+    return tree, dt
+
+
+def run_reference(args, rank, world):
+    """The reference algorithm on the host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    import numpy as np
+    from skirt7_b200 import _abi as A
+    model = build_model(args)
+    tree, _ = get_tree(args, model, 0) if _has_gpu() else (None, 0)
+    if tree is None:
+        print(json.dumps({"impl": "reference", "unavailable": "the octree is built on the device; no GPU present"}))
+        return
+    model.dustGrid = tree
+    model.rho = _density_for(model, tree)
+    threads = os.cpu_count() or 1
+    oracle.build()
+    # calibrate the sample to about --cpu-seconds per step
+    probe = oracle.simulate(model, args.packets * args.gpus, nthreads=threads, seed=1, max_packets=2000)
+    rate = probe["stats"]["packets"] / max(probe["stats"]["seconds"], 1e-6)
+    sample = int(max(1000, min(2e6, rate * args.cpu_seconds)))
+    vals = []
+    for s in range(args.warmup + args.steps):
+        r = oracle.simulate(model, args.packets * args.gpus, nthreads=threads, seed=100 + s, max_packets=sample)
+        if s >= args.warmup:
+            vals.append(r["stats"]["packets"] / r["stats"]["seconds"])
+    v = statistics.mean(vals)
+    line = {"metric": "photon packets/s (stellar emission, octree pan disk)", "value": v, "unit": "packets/s",
+            "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sample / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": _config(args, tree),
+            "cpu_baseline": {"value": v, "unit": "packets/s", "cores": threads, "kind": "port",
+                             "sample": "%d packets of the workload (all 50 wavelengths) per step" % sample},
+            "e2e": {"value": v, "unit": "packets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def _has_gpu():
+    try:
+        from skirt7_b200 import runtime
+        return runtime.device_count() > 0
+    except Exception:
+        return False
+
+
+def _density_for(model, tree):
+    """Cell densities sampled on the device (DustSystem::setSampleDensityBody), read back so the
+    CPU baseline uses the same ones."""
+    from skirt7_b200 import runtime
+    model.dustGrid = tree
+    model.rho = None
+    ctx = runtime.Context(model, 0)
+    rho = ctx.density()
+    ctx.close()
+    return rho
+
+
+def _config(args, tree):
+    return {"workload": "panchromatic octree disk galaxy: %d wavelengths 0.1-10 micron, octree max level %d, "
+                        "mass fraction %g (%d leaves), 3 frames 512x512 at 0/60/88 deg" %
+                        (args.nlambda, args.max_level, args.mass_fraction, tree.ncells if tree is not None else -1),
+            "packets_per_wavelength_per_gpu": args.packets, "nlambda": args.nlambda,
+            "cells": tree.ncells if tree is not None else None,
+            "geometry_precision": args.precision, "tallies": "fp64",
+            "l2": "working set (node records, neighbour lists, 315 MB of frames) exceeds the 126 MB L2",
+            "parallelism": "dp%d (packet ranges per GPU, NCCL all-reduce of frames per step)" % args.gpus}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    from skirt7_b200 import _abi as A
+    from skirt7_b200 import runtime
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    model = build_model(args)
+    tree, tree_s = get_tree(args, model, local)
+    model.dustGrid = tree
+    model.rho = None
+    ctx = runtime.Context(model, device=local)
+    nl = model.wavelengthGrid.Nlambda
+    ells = np.arange(nl, dtype=np.int32)
+    npp_rank = int(args.packets)
+    Npp = npp_rank * world                      # the simulation's packets per wavelength
+    first = rank * npp_rank
+    prec = A.PREC_FP64 if args.precision == "fp64" else A.PREC_FP32
+    stream = torch.cuda.current_stream(local).cuda_stream
+
+    # frames on the device for the all-reduce (N>1): a torch buffer per instrument
+    def step(seed):
+        ctx.reset_tallies()
+        ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=seed, precision=prec, stream=stream)
+
+    for w in range(args.warmup):
+        step(1000 + w)
+    torch.cuda.synchronize()
+    ctx.counters()   # also checks the error word
+
+    # ---- device-timed steps (CUDA events on the launching stream), max over ranks
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    red = None
+    if dist:
+        red = [torch.zeros(int(np.prod((1, nl, 512, 512))), dtype=torch.float64, device="cuda") for _ in range(3)]
+    step_ms_kernel = []
+    for s in range(args.steps):
+        ctx.reset_tallies()
+        ev[s][0].record()
+        ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=2000 + s, precision=prec, stream=stream)
+        if dist:
+            for t in red:
+                dist.all_reduce(t)
+        ev[s][1].record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(ms)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    torch.cuda.synchronize()
+    packets = Npp * nl * args.steps                # all ranks together
+    value = packets / (total_ms / 1e3)
+
+    # per-launch kernel time and counters of the last step for the roofline
+    ctx.reset_tallies()
+    ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=999, precision=prec)
+    ctx.sync()
+    kms = ctx.last_phase_ms()
+    c = ctx.counters()
+    # algorithmic bytes (FP32 octree, neighbour search): per cell step the cell density (4 B) and the
+    # leaf box (24 B); per scanned neighbour entry its id (4 B) and box (24 B); per tally update 8 B
+    bstep = 4 + 24 if prec == A.PREC_FP32 else 8 + 48
+    bnbr = 4 + 24 if prec == A.PREC_FP32 else 4 + 48
+    alg_bytes = c["steps"] * bstep + c["nbr_scanned"] * bnbr + 8 * (c["absorb_adds"] + c["pixel_adds"])
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (kms / 1e3) / 1e9
+
+    # ---- end to end through the C ABI with host buffers: reset, run, read the 3 frames to host
+    cubes_bytes = sum(8 * nl * 512 * 512 for _ in range(3))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        ctx.reset_tallies()
+        ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=3000 + s, precision=prec)
+        for i in range(3):
+            ctx.read_instrument(i)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = packets / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args, model, tree, ctx)
+
+    if rank == 0:
+        line = {
+            "metric": "photon packets/s (stellar emission, octree pan disk)",
+            "value": value, "unit": "packets/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if prec == A.PREC_FP32 else "f64", "data": "synthetic",
+            "config": _config(args, tree),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": kms},
+            "e2e": {"value": e2e, "unit": "packets/s", "h2d_bytes_per_step": 4 * nl + 64,
+                    "d2h_bytes_per_step": cubes_bytes},
+            "gpu_launches": args.steps,
+            "clocks": clk,
+            "counters_last_step": c,
+            "tree_build_s": tree_s,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(args, model, tree, ctx):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.build()
+    model.rho = ctx.density()
+    threads = os.cpu_count() or 1
+    probe = oracle.simulate(model, args.packets, nthreads=threads, seed=1, max_packets=2000)
+    rate = probe["stats"]["packets"] / max(probe["stats"]["seconds"], 1e-6)
+    sample = int(max(1000, min(2e6, rate * args.cpu_seconds)))
+    r = oracle.simulate(model, args.packets, nthreads=threads, seed=2, max_packets=sample)
+    model.rho = None
+    return {"value": r["stats"]["packets"] / r["stats"]["seconds"], "unit": "packets/s", "cores": threads,
+            "kind": "port", "sample": "%d packets over all %d wavelengths (%.1f s)" %
+                                      (r["stats"]["packets"], args.nlambda, r["stats"]["seconds"])}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,161 @@
+"""TEST INFRASTRUCTURE ONLY -- ctypes wrapper of the CPU oracle (oracle/liboracle.so).
+
+The oracle is a scalar FP64 restatement of SKIRT7's packet life cycle (oracle/oracle.cpp).  It
+takes the same scene structs as the CUDA library (include/skirt_b200.h) and is used by tests/,
+by __graft_entry__.smoke() as the checker and by bench.py as the CPU baseline; the product never
+imports it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+SRC = os.path.join(HERE, "oracle.cpp")
+HDR = os.path.join(HERE, "..", "include", "skirt_b200.h")
+
+dp = C.POINTER(C.c_double)
+i32p = C.POINTER(C.c_int32)
+i64p = C.POINTER(C.c_int64)
+
+
+class Stats(C.Structure):
+    _fields_ = [("packets", C.c_int64), ("steps", C.c_int64), ("traversals", C.c_int64),
+                ("scatterings", C.c_int64), ("fallbacks", C.c_int64), ("npp", C.c_uint64), ("chunks", C.c_uint64),
+                ("seconds", C.c_double)]
+
+
+def build():
+    """Compiles the oracle with the reference's floating-point semantics (no FMA contraction)."""
+    if os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(SRC), os.path.getmtime(HDR)):
+        return LIB
+    subprocess.check_call(["g++", "-O2", "-std=c++20", "-ffp-contract=off", "-fPIC", "-shared", "-o", LIB, SRC,
+                           "-lpthread"])
+    return LIB
+
+
+_lib = None
+_ref = None
+REF_LIB = os.path.join(HERE, "_ref", "libskirt_ref.so")
+
+
+def ref():
+    """The reference's own translation units (oracle/_ref), or None when they were not built."""
+    global _ref
+    if _ref is None and os.path.exists(REF_LIB):
+        R = C.CDLL(REF_LIB)
+        R.ref_pathlength.restype = C.c_double
+        R.ref_pathlength.argtypes = [dp, dp, C.c_int, C.c_double]
+        R.ref_moveinside.argtypes = [dp, C.c_double, dp, dp, dp, dp]
+        R.ref_tree_neighbors.restype = C.c_int64
+        R.ref_tree_neighbors.argtypes = [C.c_int, dp, C.POINTER(C.c_uint8), C.c_int64, C.c_int64, dp, i64p, i32p,
+                                         C.c_int64]
+        R.ref_voronoi.restype = C.c_int64
+        R.ref_voronoi.argtypes = [dp, C.c_int, dp, C.c_int, i64p, i32p, C.c_int64, dp, dp, dp]
+        R.ref_lambertw1.restype = C.c_double
+        R.ref_lambertw1.argtypes = [C.c_double]
+        R.ref_sersic.argtypes = [C.c_double, dp, C.c_int, dp, dp, dp, C.c_int, dp]
+        _ref = R
+    return _ref
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        L.orc_trace_paths.argtypes = [C.c_void_p, dp, dp, C.c_int64, i32p, dp, i64p, C.c_int64, i64p]
+        L.orc_optical_depth.argtypes = [C.c_void_p, dp, dp, C.c_int64, C.c_int, dp]
+        L.orc_pathlength.restype = C.c_double
+        L.orc_pathlength.argtypes = [dp, dp, C.c_int, C.c_double]
+        L.orc_moveinside.argtypes = [dp, C.c_double, dp, dp, dp, dp]
+        L.orc_sersic.argtypes = [C.c_double, dp, C.c_int, dp, dp, dp, C.c_int, dp]
+        L.orc_lambertw1.restype = C.c_double
+        L.orc_lambertw1.argtypes = [C.c_double]
+        L.orc_sample_positions.argtypes = [C.c_void_p, C.c_int64, C.c_uint64, dp]
+        L.orc_density.argtypes = [C.c_void_p, dp, C.c_int64, dp]
+        L.orc_sample_density.argtypes = [C.c_void_p, C.c_int, C.c_uint64, dp]
+        L.orc_chunk_params.argtypes = [C.c_double, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint64),
+                                       C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.orc_simulate.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_int64,
+                                   C.POINTER(dp), C.POINTER(dp), dp, dp, dp, C.POINTER(Stats)]
+        _lib = L
+    return _lib
+
+
+def trace_paths(model, r, k):
+    sc, keep = model.lower()
+    r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
+    k = np.ascontiguousarray(k, dtype=np.float64).reshape(-1, 3)
+    n = len(r)
+    off = np.zeros(n + 1, dtype=np.int64)
+    fb = np.zeros(1, dtype=np.int64)
+    cap = 0
+    cells = np.zeros(1, dtype=np.int32)
+    ds = np.zeros(1)
+    L = lib()
+    rc = L.orc_trace_paths(C.byref(sc), r.ctypes.data_as(dp), k.ctypes.data_as(dp), n, cells.ctypes.data_as(i32p),
+                           ds.ctypes.data_as(dp), off.ctypes.data_as(i64p), cap, fb.ctypes.data_as(i64p))
+    if rc == 8:
+        cap = int(off[n])
+        cells = np.zeros(max(cap, 1), dtype=np.int32)
+        ds = np.zeros(max(cap, 1))
+        rc = L.orc_trace_paths(C.byref(sc), r.ctypes.data_as(dp), k.ctypes.data_as(dp), n,
+                               cells.ctypes.data_as(i32p), ds.ctypes.data_as(dp), off.ctypes.data_as(i64p), cap,
+                               fb.ctypes.data_as(i64p))
+    assert rc == 0
+    tot = int(off[n])
+    return off, cells[:tot], ds[:tot]
+
+
+def optical_depth(model, r, k, ell=0):
+    sc, keep = model.lower()
+    r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
+    k = np.ascontiguousarray(k, dtype=np.float64).reshape(-1, 3)
+    tau = np.zeros(len(r))
+    assert lib().orc_optical_depth(C.byref(sc), r.ctypes.data_as(dp), k.ctypes.data_as(dp), len(r), ell,
+                                   tau.ctypes.data_as(dp)) == 0
+    return tau
+
+
+def sample_density(model, nthreads=8, seed=99):
+    sc, keep = model.lower()
+    rho = np.zeros(len(model.dustComps) * model.dustGrid.ncells)
+    lib().orc_sample_density(C.byref(sc), nthreads, seed, rho.ctypes.data_as(dp))
+    return rho.reshape(len(model.dustComps), -1)
+
+
+def simulate(model, packages, nthreads=8, seed=4357, selfabs_cycles=0, dust_emission_phase=False, max_packets=0):
+    """Runs the restated life cycle; returns dict(cubes, seds, labs_stel, labs_dust, T, stats)."""
+    sc, keep = model.lower()
+    nl = model.wavelengthGrid.Nlambda
+    ncomp = []
+    cubes, seds = [], []
+    for ins in model.instruments:
+        nc = 1 if ins.type != 3 else 6 + ins.scatteringLevels
+        ncomp.append(nc)
+        if ins.type == 0:
+            cubes.append(None)
+        else:
+            cubes.append(np.zeros((nc, nl, ins.pixelsY, ins.pixelsX)))
+        seds.append(np.zeros((nc, nl)))
+    ni = len(model.instruments)
+    cp = (dp * max(ni, 1))()
+    sp = (dp * max(ni, 1))()
+    for i in range(ni):
+        cp[i] = cubes[i].ctypes.data_as(dp) if cubes[i] is not None else None
+        sp[i] = seds[i].ctypes.data_as(dp)
+    ncells = model.dustGrid.ncells if model.dustGrid is not None else 0
+    ls = np.zeros(ncells * nl)
+    ld = np.zeros(ncells * nl)
+    T = np.zeros(max(ncells, 1))
+    st = Stats()
+    assert lib().orc_simulate(C.byref(sc), float(packages), nthreads, seed, selfabs_cycles, int(dust_emission_phase),
+                              int(max_packets), cp, sp, ls.ctypes.data_as(dp), ld.ctypes.data_as(dp),
+                              T.ctypes.data_as(dp), C.byref(st)) == 0
+    stats = {n: getattr(st, n) for n, _ in Stats._fields_}
+    return dict(cubes=cubes, seds=seds, labs_stel=ls.reshape(ncells, nl), labs_dust=ld.reshape(ncells, nl),
+                T=T[:ncells], stats=stats)

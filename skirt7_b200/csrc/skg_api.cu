@@ -1,0 +1,906 @@
+// skg_api.cu -- the C ABI (include/skirt_b200.h): contexts, scene upload, phase launches,
+// tallies, the bit-exact path harness and the grid builders.
+#include "skg_scene.cuh"
+#include "skg_internal.h"
+#include "skg_tree.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <thread>
+#include <vector>
+
+using namespace skg;
+
+namespace {
+
+struct Allocs {
+    std::vector<void*> ptrs;
+    size_t bytes = 0;
+    ~Allocs() { release(); }
+    void release() { for (void* p : ptrs) cudaFree(p); ptrs.clear(); bytes = 0; }
+    template<typename T> T* alloc(size_t n) {
+        if (n == 0) n = 1;
+        void* p = nullptr;
+        if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+        ptrs.push_back(p); bytes += n * sizeof(T);
+        return (T*)p;
+    }
+};
+
+struct Failure { int code; std::string msg; };
+#define CK(expr) do { cudaError_t e_ = (expr); if (e_ != cudaSuccess) throw Failure{SKG_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)}; } while (0)
+#define REQUIRE(cond, msg) do { if (!(cond)) throw Failure{SKG_ERR_INVALID, msg}; } while (0)
+
+template<typename T> T* upload(Allocs& A, const T* h, size_t n, cudaStream_t s) {
+    T* d = A.alloc<T>(n);
+    if (!d) throw Failure{SKG_ERR_OOM, "device allocation failed"};
+    if (h && n) CK(cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+    return d;
+}
+template<typename T> T* zeros(Allocs& A, size_t n, cudaStream_t s) {
+    T* d = A.alloc<T>(n);
+    if (!d) throw Failure{SKG_ERR_OOM, "device allocation failed"};
+    CK(cudaMemsetAsync(d, 0, std::max<size_t>(n, 1) * sizeof(T), s));
+    return d;
+}
+
+// cubic spline kernel cumulative mass table (CubicSplineSmoothingKernel.cpp:22-38)
+std::vector<double> cubic_spline_table() {
+    const int Nu = 400;
+    std::vector<double> X(Nu + 1);
+    for (int k = 0; k <= Nu; k++) {
+        double u = k * (1.0 / Nu), u2 = u * u, u3 = u * u2;
+        X[k] = (u < 0.5) ? u3 * (32.0 / 3.0 - 192.0 / 5.0 * u2 + 32.0 * u3)
+                         : -1.0 / 15.0 - 64.0 * u3 * (-1.0 / 3.0 + 0.75 * u - 0.6 * u2 + u3 / 6.0);
+    }
+    return X;
+}
+
+// Builds the device form of a geometry (tables uploaded into A).
+DevGeometry make_geometry(Allocs& A, const skg_geometry& g, cudaStream_t s) {
+    DevGeometry G;
+    std::memset(&G, 0, sizeof(G));
+    G.type = g.type;
+    for (int i = 0; i < 6; i++) G.p[i] = g.p[i];
+    if (g.type == SKG_GEOM_EXPDISK) {
+        // ExpDiskGeometry::setupSelfBefore (ExpDiskGeometry.cpp:24-40)
+        G.hR = g.p[0]; G.hz = g.p[1]; G.Rmax = g.p[2]; G.zmax = g.p[3]; G.Rmin = g.p[4];
+        REQUIRE(G.hR > 0 && G.hz > 0, "exponential disk scale lengths must be positive");
+        double intz = (G.zmax > 0) ? -2.0 * G.hz * std::expm1(-G.zmax / G.hz) : 2.0 * G.hz;
+        double tmin = (G.Rmin > 0) ? std::exp(-G.Rmin / G.hR) * (1.0 + G.Rmin / G.hR) : 1.0;
+        double tmax = (G.Rmax > 0) ? std::exp(-G.Rmax / G.hR) * (1.0 + G.Rmax / G.hR) : 0.0;
+        G.rho0 = 1.0 / (G.hR * G.hR * (tmin - tmax) * 2.0 * M_PI * intz);
+    } else if (g.type == SKG_GEOM_SERSIC) {
+        REQUIRE(g.p[0] > 0.5 && g.p[0] <= 10 && g.p[1] > 0, "Sersic index must be in (0.5,10] and radius positive");
+        std::vector<double> sv(101), Sv(101), Mv(101);
+        sersic_table(g.p[0], sv.data(), Sv.data(), Mv.data());
+        G.sv = upload(A, sv.data(), 101, s); G.Sv = upload(A, Sv.data(), 101, s); G.Mv = upload(A, Mv.data(), 101, s);
+        G.reff = g.p[1]; G.srho0 = 1.0 / (G.reff * G.reff * G.reff);
+    } else if (g.type == SKG_GEOM_PLUMMER) {
+        REQUIRE(g.p[0] > 0, "Plummer scale radius must be positive");
+    } else {
+        REQUIRE(g.type == SKG_GEOM_POINT, "unknown geometry type");
+    }
+    if (g.clump_count > 0) {
+        REQUIRE(g.clump_pos != nullptr, "clumpy geometry needs clump positions");
+        REQUIRE(g.clump_fraction >= 0 && g.clump_fraction <= 1 && g.clump_radius > 0, "invalid clump parameters");
+        G.f = g.clump_fraction; G.N = g.clump_count; G.h = g.clump_radius; G.cutoff = g.clump_cutoff;
+        G.kernel = g.clump_kernel;
+        std::vector<int> idx(G.N);
+        for (int i = 0; i < G.N; i++) idx[i] = i;
+        std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return g.clump_pos[3 * a] < g.clump_pos[3 * b]; });
+        std::vector<double> cl(3 * (size_t)G.N);
+        for (int i = 0; i < G.N; i++) for (int c = 0; c < 3; c++) cl[3 * i + c] = g.clump_pos[3 * idx[i] + c];
+        G.clumps = upload(A, cl.data(), cl.size(), s);
+        std::vector<double> kx = cubic_spline_table();
+        G.kXv = upload(A, kx.data(), kx.size(), s);
+    }
+    return G;
+}
+
+double grid_diag(const skg_grid& g) {
+    double dx = g.xmax - g.xmin, dy = g.ymax - g.ymin, dz = g.zmax - g.zmin;
+    return std::sqrt(dx * dx + dy * dy + dz * dz);
+}
+
+int64_t grid_ncells(const skg_grid& g) {
+    if (g.type == SKG_GRID_CARTESIAN) return (int64_t)g.nx * g.ny * g.nz;
+    if (g.type == SKG_GRID_VORONOI) return g.nsites;
+    int64_t c = 0;
+    for (int l = 0; l < g.nnodes; l++) if (g.node_cell[l] >= 0) c++;
+    return c;
+}
+
+// Uploads a grid into both precisions.
+DevGrid make_grid(Allocs& A, const skg_grid& g, cudaStream_t s) {
+    DevGrid G;
+    std::memset(&G, 0, sizeof(G));
+    G.type = g.type;
+    G.xmin = g.xmin; G.ymin = g.ymin; G.zmin = g.zmin; G.xmax = g.xmax; G.ymax = g.ymax; G.zmax = g.zmax;
+    REQUIRE(g.xmax > g.xmin && g.ymax > g.ymin && g.zmax > g.zmin, "grid extent is empty");
+    double diag = grid_diag(g);
+    G.eps = 1e-12 * diag;
+    double amax = std::max({std::fabs(g.xmin), std::fabs(g.xmax), std::fabs(g.ymin), std::fabs(g.ymax),
+                            std::fabs(g.zmin), std::fabs(g.zmax)});
+    // FP32 nudge: four units in the last place of the largest coordinate
+    G.epsf = (float)std::max(4.0 * amax * std::ldexp(1.0, -23), 1e-12 * diag);
+    G.max_steps = 1 << 20;
+    if (g.type == SKG_GRID_CARTESIAN) {
+        REQUIRE(g.nx > 0 && g.ny > 0 && g.nz > 0 && g.xv && g.yv && g.zv, "Cartesian grid needs planes");
+        REQUIRE((int64_t)g.nx * g.ny * g.nz < (1ll << 31), "too many Cartesian cells");
+        G.nx = g.nx; G.ny = g.ny; G.nz = g.nz;
+        G.xv = upload(A, g.xv, g.nx + 1, s); G.yv = upload(A, g.yv, g.ny + 1, s); G.zv = upload(A, g.zv, g.nz + 1, s);
+        std::vector<float> f;
+        f.assign(g.xv, g.xv + g.nx + 1); G.xvf = upload(A, f.data(), f.size(), s);
+        f.assign(g.yv, g.yv + g.ny + 1); G.yvf = upload(A, f.data(), f.size(), s);
+        f.assign(g.zv, g.zv + g.nz + 1); G.zvf = upload(A, f.data(), f.size(), s);
+        G.ncells = g.nx * g.ny * g.nz;
+    } else if (g.type == SKG_GRID_OCTREE || g.type == SKG_GRID_BINTREE) {
+        int n = g.nnodes;
+        REQUIRE(n > 0 && g.node_box && g.node_child && g.node_father && g.node_cell && g.node_dir, "tree grid needs node arrays");
+        G.nnodes = n;
+        G.node_box = upload(A, g.node_box, 6 * (size_t)n, s);
+        G.node_child = upload(A, g.node_child, n, s);
+        G.node_father = upload(A, g.node_father, n, s);
+        G.node_cell = upload(A, g.node_cell, n, s);
+        G.node_dir = upload(A, (const signed char*)g.node_dir, n, s);
+        std::vector<float4> nf(2 * (size_t)n);
+        int nc = 0;
+        for (int l = 0; l < n; l++) {
+            const double* b = g.node_box + 6 * (size_t)l;
+            int ch = g.node_child[l], ce = g.node_cell[l];
+            float4 a, c;
+            a.x = (float)b[0]; a.y = (float)b[1]; a.z = (float)b[2]; std::memcpy(&a.w, &ch, 4);
+            c.x = (float)b[3]; c.y = (float)b[4]; c.z = (float)b[5]; std::memcpy(&c.w, &ce, 4);
+            nf[2 * l] = a; nf[2 * l + 1] = c;
+            if (ce >= 0) nc++;
+        }
+        G.nodef = upload(A, nf.data(), nf.size(), s);
+        std::vector<int> cn(nc);
+        for (int l = 0; l < n; l++) if (g.node_cell[l] >= 0) {
+            REQUIRE(g.node_cell[l] < nc, "leaf cell number out of range");
+            cn[g.node_cell[l]] = l;
+        }
+        G.cell_node = upload(A, cn.data(), cn.size(), s);
+        G.ncells = nc;
+        G.search = g.search_method;
+        if (g.search_method == SKG_SEARCH_NEIGHBOR) {
+            REQUIRE(g.nbr_offsets && g.nbr_ids, "neighbour search needs neighbour lists");
+            int64_t tot = g.nbr_offsets[6 * (size_t)n];
+            REQUIRE(tot < (1ll << 31), "too many neighbour entries");
+            std::vector<int> off(6 * (size_t)n + 1);
+            for (size_t q = 0; q <= 6 * (size_t)n; q++) off[q] = (int)g.nbr_offsets[q];
+            G.nbroff = upload(A, off.data(), off.size(), s);
+            G.nbr = upload(A, g.nbr_ids, (size_t)tot, s);
+        }
+        REQUIRE(g.search_method != SKG_SEARCH_BOOKKEEPING || g.type == SKG_GRID_OCTREE,
+                "the bookkeeping search method requires an octree");
+    } else if (g.type == SKG_GRID_VORONOI) {
+        int n = g.nsites;
+        REQUIRE(n > 0 && g.sites && g.vnbr_offsets && g.vnbr_ids && g.nb > 0 && g.block_offsets && g.block_ids,
+                "Voronoi grid needs sites, neighbour lists and block lists");
+        G.nsites = n; G.ncells = n;
+        G.site = upload(A, g.sites, 3 * (size_t)n, s);
+        std::vector<float4> sf(n);
+        for (int m = 0; m < n; m++) sf[m] = make_float4((float)g.sites[3 * m], (float)g.sites[3 * m + 1], (float)g.sites[3 * m + 2], 0.f);
+        G.sitef = upload(A, sf.data(), sf.size(), s);
+        int64_t tot = g.vnbr_offsets[n];
+        REQUIRE(tot < (1ll << 31), "too many Voronoi neighbour entries");
+        std::vector<int> off(n + 1);
+        for (int m = 0; m <= n; m++) off[m] = (int)g.vnbr_offsets[m];
+        G.vnoff = upload(A, off.data(), off.size(), s);
+        G.vnbr = upload(A, g.vnbr_ids, (size_t)tot, s);
+        // FP32 bisector planes: n = p_i - p_r, w = n . (p_i + p_r)/2 (computed in FP64, stored FP32);
+        // walls -1..-6 as axis planes with outward normals
+        std::vector<float4> pl((size_t)tot);
+        for (int m = 0; m < n; m++) {
+            const double* pr = g.sites + 3 * (size_t)m;
+            for (int64_t q = g.vnbr_offsets[m]; q < g.vnbr_offsets[m + 1]; q++) {
+                int mi = g.vnbr_ids[q];
+                double nx, ny, nz, w;
+                if (mi >= 0) {
+                    REQUIRE(mi < n, "Voronoi neighbour id out of range");
+                    const double* pi = g.sites + 3 * (size_t)mi;
+                    nx = pi[0] - pr[0]; ny = pi[1] - pr[1]; nz = pi[2] - pr[2];
+                    w = nx * 0.5 * (pi[0] + pr[0]) + ny * 0.5 * (pi[1] + pr[1]) + nz * 0.5 * (pi[2] + pr[2]);
+                } else {
+                    nx = ny = nz = 0;
+                    switch (mi) {
+                        case -1: nx = -1; w = -g.xmin; break;
+                        case -2: nx = 1;  w = g.xmax; break;
+                        case -3: ny = -1; w = -g.ymin; break;
+                        case -4: ny = 1;  w = g.ymax; break;
+                        case -5: nz = -1; w = -g.zmin; break;
+                        case -6: nz = 1;  w = g.zmax; break;
+                        default: throw Failure{SKG_ERR_INVALID, "invalid Voronoi wall id"};
+                    }
+                }
+                pl[q] = make_float4((float)nx, (float)ny, (float)nz, (float)w);
+            }
+        }
+        G.vplane = upload(A, pl.data(), pl.size(), s);
+        G.nb = g.nb;
+        size_t nb3 = (size_t)g.nb * g.nb * g.nb;
+        int64_t btot = g.block_offsets[nb3];
+        REQUIRE(btot < (1ll << 31), "too many block list entries");
+        std::vector<int> boff(nb3 + 1);
+        for (size_t b = 0; b <= nb3; b++) boff[b] = (int)g.block_offsets[b];
+        G.boff = upload(A, boff.data(), boff.size(), s);
+        G.bids = upload(A, g.block_ids, (size_t)btot, s);
+        if (g.cell_bbox) G.vbbox = upload(A, g.cell_bbox, 6 * (size_t)n, s);
+        else {
+            std::vector<double> bb(6 * (size_t)n);
+            for (int m = 0; m < n; m++) { bb[6*m] = g.xmin; bb[6*m+1] = g.ymin; bb[6*m+2] = g.zmin; bb[6*m+3] = g.xmax; bb[6*m+4] = g.ymax; bb[6*m+5] = g.zmax; }
+            G.vbbox = upload(A, bb.data(), bb.size(), s);
+        }
+        if (g.cell_volume) G.vvol = upload(A, g.cell_volume, n, s);
+        else G.vvol = zeros<double>(A, n, s);
+    } else {
+        throw Failure{SKG_ERR_INVALID, "unknown grid type"};
+    }
+    return G;
+}
+
+double planck_B(double lambda, double T) {   // PlanckFunction.cpp:24-33
+    const double h = 6.62606957e-34, c = 2.99792458e8, k = 1.3806488e-23;
+    double x = h * c / (lambda * k * T);
+    return 2.0 * h * c * c / std::pow(lambda, 5) / (std::exp(x) - 1.0);
+}
+
+}  // namespace
+
+struct skg_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0;
+    Allocs A;
+    DevGrid grid;
+    DevScene hs;
+    DevScene* ds = nullptr;
+    int nlambda = 0, ncomp = 0;
+    int64_t ncells = 0;
+    std::vector<int64_t> cube_len, sed_len;
+    unsigned long long* counters = nullptr;
+    unsigned* err = nullptr;
+    unsigned long long* work = nullptr;
+    int* ells = nullptr; int ells_cap = 0;
+    std::vector<double> lambda, dlambda;
+    // dust emission
+    int nT = 0;
+    double *Tv = nullptr, *planckabs = nullptr, *labsbol = nullptr, *spectra = nullptr, *temperature = nullptr;
+    double *emit_Lv = nullptr, *emit_cdf = nullptr, *emit_Ltot = nullptr, *sumbuf = nullptr;
+    void* scan_scratch = nullptr; size_t scan_bytes = 0;
+    std::string error;
+};
+
+static int fail(skg_ctx* ctx, const Failure& f) {
+    set_error(f.msg);
+    if (ctx) ctx->error = f.msg;
+    return f.code;
+}
+
+extern "C" {
+
+int skg_version(void) { return SKG_ABI_VERSION; }
+
+const char* skg_last_error(const skg_ctx* ctx) {
+    if (ctx && !ctx->error.empty()) return ctx->error.c_str();
+    return get_error();
+}
+
+int skg_device_count(int* count) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) { cudaGetLastError(); *count = 0; set_error(cudaGetErrorString(e)); return SKG_ERR_NO_DEVICE; }
+    *count = n;
+    return SKG_OK;
+}
+
+int skg_chunk_params(double packages, int nthreads, int nprocs, int nlambda,
+                     uint64_t* nchunks, uint64_t* chunksize, uint64_t* npp) {
+    chunk_params(packages, nthreads, nprocs, nlambda, *nchunks, *chunksize, *npp);
+    return SKG_OK;
+}
+
+int skg_ctx_create(const skg_scene* sc, int device, skg_ctx** out) {
+    *out = nullptr;
+    skg_ctx* ctx = new skg_ctx();
+    try {
+        REQUIRE(sc != nullptr, "scene is null");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); throw Failure{SKG_ERR_NO_DEVICE, "no CUDA device"}; }
+        REQUIRE(device >= 0 && device < ndev, "device index out of range");
+        ctx->device = device;
+        CK(cudaSetDevice(device));
+        CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&ctx->ev0)); CK(cudaEventCreate(&ctx->ev1));
+        cudaStream_t s = ctx->stream;
+        Allocs& A = ctx->A;
+
+        REQUIRE(sc->nlambda > 0 && sc->lambda && sc->dlambda, "wavelength grid is empty");
+        REQUIRE(sc->ncomp >= 0 && sc->ncomp <= MAX_COMP, "at most 4 dust components");
+        REQUIRE(sc->nstellar >= 1 && sc->nstellar <= MAX_STELLAR, "1..8 stellar components");
+        REQUIRE(sc->ninstr >= 0 && sc->ninstr <= MAX_INSTR, "at most 16 instruments");
+        REQUIRE(sc->scatt_bias >= 0 && sc->scatt_bias <= 1, "The scattering bias should be between 0 and 1");
+        REQUIRE(sc->min_weight_reduction == 0 || sc->min_weight_reduction >= 1e3,
+                "The minimum weight reduction factor should be larger than 1000");
+        REQUIRE(sc->min_scatt_events >= 0 && sc->min_scatt_events <= 1000, "minScattEvents out of range");
+        const int nl = sc->nlambda;
+        ctx->nlambda = nl; ctx->ncomp = sc->ncomp;
+        ctx->lambda.assign(sc->lambda, sc->lambda + nl);
+        ctx->dlambda.assign(sc->dlambda, sc->dlambda + nl);
+
+        DevScene& H = ctx->hs;
+        std::memset(&H, 0, sizeof(H));
+        ctx->grid = make_grid(A, sc->grid, s);
+        ctx->ncells = ctx->grid.ncells;
+        const int64_t nc = ctx->ncells;
+        H.ncells = (int)nc;
+        H.nlambda = nl;
+        H.lambda = upload(A, sc->lambda, nl, s);
+        H.dlambda = upload(A, sc->dlambda, nl, s);
+
+        // dust mixes (SimpleOligoDustMix.cpp:38-45: kappa_abs = kappa_ext(1-a), kappa_sca = kappa_ext a)
+        H.ncomp = sc->ncomp;
+        if (sc->ncomp > 0) {
+            std::vector<double> ke(sc->ncomp * nl), ks(sc->ncomp * nl), al(sc->ncomp * nl), gg(sc->ncomp * nl);
+            std::vector<DevGeometry> dg(sc->ncomp);
+            std::vector<double> norms(sc->ncomp);
+            for (int h = 0; h < sc->ncomp; h++) {
+                const skg_dust_comp& d = sc->dust[h];
+                REQUIRE(d.kappaext && d.albedo && d.asymmpar, "dust mix tables missing");
+                for (int l = 0; l < nl; l++) {
+                    ke[h * nl + l] = d.kappaext[l]; al[h * nl + l] = d.albedo[l]; gg[h * nl + l] = d.asymmpar[l];
+                    ks[h * nl + l] = d.kappaext[l] * d.albedo[l];
+                    REQUIRE(d.kappaext[l] >= 0 && d.albedo[l] >= 0 && d.albedo[l] <= 1 && std::fabs(d.asymmpar[l]) < 1,
+                            "invalid dust mix values");
+                }
+                if (!sc->rho) dg[h] = make_geometry(A, d.geometry, s);
+                norms[h] = d.norm;
+            }
+            H.kext = upload(A, ke.data(), ke.size(), s);
+            H.ksca = upload(A, ks.data(), ks.size(), s);
+            H.albedo = upload(A, al.data(), al.size(), s);
+            H.asym = upload(A, gg.data(), gg.size(), s);
+            double* rho;
+            if (sc->rho) {
+                for (int64_t i = 0; i < nc * sc->ncomp; i++)
+                    REQUIRE(sc->rho[i] >= 0 && std::isfinite(sc->rho[i]), "cell densities must be finite and non-negative");
+                rho = upload(A, sc->rho, (size_t)(nc * sc->ncomp), s);
+            } else {
+                // DustSystem::setSampleDensityBody on the device
+                rho = A.alloc<double>(nc * sc->ncomp);
+                if (!rho) throw Failure{SKG_ERR_OOM, "device allocation failed"};
+                DevGeometry* dgd = upload(A, dg.data(), dg.size(), s);
+                double* nd = upload(A, norms.data(), norms.size(), s);
+                CK(launch_sample_density(ctx->grid, nullptr, dgd, nd, sc->ncomp,
+                                         sc->density_samples > 0 ? sc->density_samples : 100, 0x5EED0001ull, rho, s));
+            }
+            H.rho = rho;
+            float* rf = A.alloc<float>(nc * sc->ncomp);
+            if (!rf) throw Failure{SKG_ERR_OOM, "device allocation failed"};
+            {
+                std::vector<double> hr(nc * sc->ncomp);
+                CK(cudaMemcpyAsync(hr.data(), rho, hr.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+                CK(cudaStreamSynchronize(s));
+                std::vector<float> hf(hr.begin(), hr.end());
+                CK(cudaMemcpyAsync(rf, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+                CK(cudaStreamSynchronize(s));
+            }
+            H.rhof = rf;
+        }
+
+        // stellar system (StellarSystem.cpp:35-52)
+        H.nstellar = sc->nstellar;
+        std::vector<double> starL(sc->nstellar * nl), Lv(nl, 0.0), Xvv((size_t)nl * (sc->nstellar + 1), 0.0);
+        for (int h = 0; h < sc->nstellar; h++) {
+            REQUIRE(sc->stellar[h].luminosity, "stellar luminosities missing");
+            H.stellar[h] = make_geometry(A, sc->stellar[h].geometry, s);
+            for (int l = 0; l < nl; l++) {
+                starL[h * nl + l] = sc->stellar[h].luminosity[l];
+                REQUIRE(starL[h * nl + l] >= 0, "stellar luminosity must be non-negative");
+            }
+        }
+        for (int l = 0; l < nl; l++) {
+            double* X = &Xvv[(size_t)l * (sc->nstellar + 1)];
+            for (int h = 0; h < sc->nstellar; h++) { Lv[l] += starL[h * nl + l]; X[h + 1] = X[h] + starL[h * nl + l]; }
+            double t = X[sc->nstellar];
+            for (int h = 0; h <= sc->nstellar; h++) X[h] = (t > 0) ? X[h] / t : 0.0;
+        }
+        H.starL = upload(A, starL.data(), starL.size(), s);
+        H.Lv = upload(A, Lv.data(), Lv.size(), s);
+        H.Xvv = upload(A, Xvv.data(), Xvv.size(), s);
+        H.emission_bias = sc->emission_bias;
+
+        // instruments (DistantInstrument.cpp:27-50, SingleFrameInstrument.cpp:26-42)
+        H.ninstr = sc->ninstr;
+        ctx->cube_len.assign(sc->ninstr, 0); ctx->sed_len.assign(sc->ninstr, 0);
+        for (int i = 0; i < sc->ninstr; i++) {
+            const skg_instrument& in = sc->instr[i];
+            DevInstr& I = H.instr[i];
+            std::memset(&I, 0, sizeof(I));
+            REQUIRE(in.distance > 0, "Distance was not set");
+            I.type = in.type;
+            I.costheta = std::cos(in.inclination); I.sintheta = std::sin(in.inclination);
+            I.cosphi = std::cos(in.azimuth); I.sinphi = std::sin(in.azimuth);
+            I.cospa = std::cos(in.position_angle); I.sinpa = std::sin(in.position_angle);
+            // Direction(theta, phi) (Direction.cpp:12-38)
+            double th = in.inclination, ph = in.azimuth;
+            if (th <= 1e-8) { I.kx = 0; I.ky = 0; I.kz = 1; }
+            else if (th >= M_PI - 1e-8) { I.kx = 0; I.ky = 0; I.kz = -1; }
+            else { I.kx = std::sin(th) * std::cos(ph); I.ky = std::sin(th) * std::sin(ph); I.kz = std::cos(th); }
+            I.ncomp = 1;
+            if (in.type == SKG_INSTR_FULL) { REQUIRE(in.nscatt_levels >= 0, "scattering levels must be >= 0"); I.nscatt_levels = in.nscatt_levels; I.ncomp = SKG_FULL_NBASE + in.nscatt_levels; }
+            if (in.type != SKG_INSTR_SED) {
+                REQUIRE(in.type == SKG_INSTR_FRAME || in.type == SKG_INSTR_SIMPLE || in.type == SKG_INSTR_FULL, "unknown instrument type");
+                REQUIRE(in.nxp > 0 && in.nyp > 0, "Number of pixels was not set");
+                REQUIRE(in.fovx > 0 && in.fovy > 0, "Field of view was not set");
+                I.nxp = in.nxp; I.nyp = in.nyp;
+                I.xpmin = in.xc - 0.5 * in.fovx; I.xpsiz = in.fovx / in.nxp;
+                I.ypmin = in.yc - 0.5 * in.fovy; I.ypsiz = in.fovy / in.nyp;
+                ctx->cube_len[i] = (int64_t)I.ncomp * nl * in.nxp * in.nyp;
+                I.cube = zeros<double>(A, ctx->cube_len[i], s);
+            }
+            ctx->sed_len[i] = (int64_t)I.ncomp * nl;
+            I.sed = zeros<double>(A, ctx->sed_len[i], s);
+        }
+        // direction groups: instruments with the same observer direction share one peel-off traversal
+        {
+            int ng = 0, pos = 0;
+            std::vector<int> assigned(sc->ninstr, -1);
+            for (int i = 0; i < sc->ninstr; i++) {
+                if (assigned[i] >= 0) continue;
+                H.group_start[ng] = pos;
+                H.gkx[ng] = H.instr[i].kx; H.gky[ng] = H.instr[i].ky; H.gkz[ng] = H.instr[i].kz;
+                bool frame_only = true;
+                for (int j = i; j < sc->ninstr; j++) {
+                    if (assigned[j] >= 0) continue;
+                    if (j == i || (H.instr[j].kx == H.instr[i].kx && H.instr[j].ky == H.instr[i].ky && H.instr[j].kz == H.instr[i].kz)) {
+                        assigned[j] = ng; H.group_instr[pos++] = j;
+                        if (H.instr[j].type != SKG_INSTR_FRAME) frame_only = false;
+                    }
+                }
+                H.group_frame_only[ng] = frame_only;
+                ng++;
+            }
+            H.group_start[ng] = pos;
+            H.ngroups = ng;
+        }
+
+        H.min_weight_reduction = sc->min_weight_reduction > 0 ? sc->min_weight_reduction : 1e4;
+        H.min_scatt_events = sc->min_scatt_events;
+        H.xi = sc->scatt_bias;
+        H.store_abs = (sc->store_absorption || sc->dust_emission) ? 1 : 0;
+        if (sc->ncomp > 0 && (sc->store_absorption || sc->dust_emission)) {
+            H.labs_stel = zeros<double>(A, (size_t)nc * nl, s);
+            H.labs_dust = zeros<double>(A, (size_t)nc * nl, s);
+        }
+        H.dust_emission_bias = sc->dust_emission_bias;
+
+        if (sc->dust_emission && sc->ncomp > 0) {
+            REQUIRE(sc->ncomp == 1, "dust emission supports one dust component");
+            // temperature grid NR::powgrid(0, 5000, 1000, 500) and Planck-integrated absorption
+            // (DustMix.cpp:239-263), with kappa_abs of the mix (the 1/mu factors cancel)
+            const int NT = 1000;
+            std::vector<double> Tv(NT + 1), pa(NT + 1, 0.0);
+            double q = std::pow(500.0, 1. / (NT - 1)), qn = std::pow(q, NT);
+            for (int i = 0; i <= NT; ++i) Tv[i] = (1. - std::pow(q, i)) / (1. - qn) * 5000.0;
+            for (int p = 1; p <= NT; p++) {
+                double acc = 0;
+                for (int l = 0; l < nl; l++) {
+                    double kabs = sc->dust[0].kappaext[l] * (1.0 - sc->dust[0].albedo[l]);
+                    acc += kabs * planck_B(sc->lambda[l], Tv[p]) * sc->dlambda[l];
+                }
+                pa[p] = acc;
+            }
+            ctx->nT = NT + 1;
+            ctx->Tv = upload(A, Tv.data(), Tv.size(), s);
+            ctx->planckabs = upload(A, pa.data(), pa.size(), s);
+            ctx->labsbol = zeros<double>(A, nc, s);
+            ctx->spectra = zeros<double>(A, (size_t)nc * nl, s);
+            ctx->temperature = zeros<double>(A, nc, s);
+            ctx->emit_Lv = zeros<double>(A, (size_t)nc * nl, s);
+            ctx->emit_cdf = zeros<double>(A, (size_t)(nc + 1) * nl, s);
+            ctx->emit_Ltot = zeros<double>(A, nl, s);
+            ctx->scan_bytes = emission_scan_scratch_bytes((int)nc);
+            ctx->scan_scratch = A.alloc<char>(ctx->scan_bytes);
+            H.emit_Lv = ctx->emit_Lv; H.emit_cdf = ctx->emit_cdf; H.emit_Ltot = ctx->emit_Ltot;
+        }
+        ctx->sumbuf = zeros<double>(A, 2, s);
+        ctx->counters = zeros<unsigned long long>(A, 10, s);
+        ctx->err = zeros<unsigned>(A, 1, s);
+        ctx->work = zeros<unsigned long long>(A, 1, s);
+        ctx->ds = upload(A, &H, 1, s);
+        CK(cudaStreamSynchronize(s));
+        *out = ctx;
+        return SKG_OK;
+    } catch (const Failure& f) {
+        int rc = fail(ctx, f);
+        set_error(f.msg);
+        if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+        ctx->A.release();
+        if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+        if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return rc;
+    }
+}
+
+int skg_ctx_destroy(skg_ctx* ctx) {
+    if (!ctx) return SKG_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->A.release();
+    cudaEventDestroy(ctx->ev0); cudaEventDestroy(ctx->ev1);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return SKG_OK;
+}
+
+int skg_ctx_info(const skg_ctx* ctx, int64_t* ncells, int64_t* device_bytes) {
+    if (!ctx) return SKG_ERR_INVALID;
+    if (ncells) *ncells = ctx->ncells;
+    if (device_bytes) *device_bytes = (int64_t)ctx->A.bytes;
+    return SKG_OK;
+}
+
+int skg_sync(skg_ctx* ctx, int timeout_ms) {
+    if (!ctx) return SKG_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    auto t0 = std::chrono::steady_clock::now();
+    while (true) {
+        cudaError_t e = cudaStreamQuery(ctx->stream);
+        if (e == cudaSuccess) break;
+        if (e != cudaErrorNotReady) { cudaGetLastError(); return fail(ctx, Failure{SKG_ERR_CUDA, cudaGetErrorString(e)}); }
+        if (timeout_ms >= 0 && std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() > timeout_ms)
+            return fail(ctx, Failure{SKG_ERR_TIMEOUT, "timed out waiting for the device"});
+        std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+    unsigned err = 0;
+    cudaMemcpy(&err, ctx->err, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    if (err & ERR_NAN_TAU) return fail(ctx, Failure{SKG_ERR_NAN_TAU, "The optical depth along the path is not a positive number"});
+    if (err & (ERR_STEP_BUDGET | ERR_SCATT_BUDGET)) return fail(ctx, Failure{SKG_ERR_STEP_BUDGET, "a packet exceeded its step or scattering budget"});
+    if (err & ERR_CAPACITY) return fail(ctx, Failure{SKG_ERR_CAPACITY, "segment buffer too small"});
+    return SKG_OK;
+}
+
+int skg_read_density(skg_ctx* ctx, double* rho) {
+    if (!ctx || !rho) return SKG_ERR_INVALID;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        if (ctx->ncomp == 0) return SKG_OK;
+        CK(cudaMemcpyAsync(rho, ctx->hs.rho, (size_t)ctx->ncells * ctx->ncomp * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        return SKG_OK;
+    } catch (const Failure& f) { return fail(ctx, f); }
+}
+
+int skg_trace_paths(skg_ctx* ctx, const double* r, const double* k, int64_t n, int precision,
+                    int32_t* cells, double* ds, int64_t* offsets, int64_t capacity) {
+    if (!ctx || n < 0 || !offsets) return SKG_ERR_INVALID;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t s = ctx->stream;
+        Allocs T;
+        double* dr = upload(T, r, 3 * (size_t)n, s);
+        double* dk = upload(T, k, 3 * (size_t)n, s);
+        int64_t* cnt = T.alloc<int64_t>(n + 1);
+        if (!cnt) throw Failure{SKG_ERR_OOM, "device allocation failed"};
+        CK(cudaMemsetAsync(ctx->err, 0, sizeof(unsigned), s));
+        CK(launch_count_segments(ctx->grid, dr, dk, n, precision, cnt, ctx->err, s));
+        std::vector<int64_t> hc(n);
+        if (n) CK(cudaMemcpyAsync(hc.data(), cnt, n * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        offsets[0] = 0;
+        for (int64_t i = 0; i < n; i++) offsets[i + 1] = offsets[i] + hc[i];
+        int64_t tot = offsets[n];
+        if (tot > capacity) throw Failure{SKG_ERR_CAPACITY, "segment buffers too small"};
+        int64_t* doff = upload(T, offsets, n + 1, s);
+        int32_t* dc = T.alloc<int32_t>(tot);
+        double* dd = T.alloc<double>(tot);
+        if (!dc || !dd) throw Failure{SKG_ERR_OOM, "device allocation failed"};
+        CK(launch_write_segments(ctx->grid, dr, dk, n, precision, doff, dc, dd, ctx->err, s));
+        if (tot) {
+            CK(cudaMemcpyAsync(cells, dc, tot * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(ds, dd, tot * sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
+        CK(cudaStreamSynchronize(s));
+        unsigned err = 0;
+        CK(cudaMemcpy(&err, ctx->err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        if (err & ERR_STEP_BUDGET) throw Failure{SKG_ERR_STEP_BUDGET, "a path exceeded the step budget"};
+        if (err & ERR_CAPACITY) throw Failure{SKG_ERR_CAPACITY, "segment count changed between passes"};
+        return SKG_OK;
+    } catch (const Failure& f) { return fail(ctx, f); }
+}
+
+int skg_optical_depth(skg_ctx* ctx, const double* r, const double* k, int64_t n, int ell, int precision, double* tau) {
+    if (!ctx || n < 0 || ell < 0 || ell >= ctx->nlambda) return SKG_ERR_INVALID;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t s = ctx->stream;
+        Allocs T;
+        double* dr = upload(T, r, 3 * (size_t)n, s);
+        double* dk = upload(T, k, 3 * (size_t)n, s);
+        double* dt = T.alloc<double>(n);
+        CK(cudaMemsetAsync(ctx->err, 0, sizeof(unsigned), s));
+        CK(launch_optical_depth(ctx->grid, ctx->ds, dr, dk, n, ell, precision, dt, ctx->err, s));
+        if (n) CK(cudaMemcpyAsync(tau, dt, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return SKG_OK;
+    } catch (const Failure& f) { return fail(ctx, f); }
+}
+
+int skg_run_phase(skg_ctx* ctx, int phase, const int32_t* ells, int nell, uint64_t npp, uint64_t first_packet,
+                  uint64_t count, uint64_t seed, const skg_run_opts* opts, void* stream) {
+    if (!ctx) return SKG_ERR_INVALID;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        REQUIRE(phase >= SKG_PHASE_STELLAR && phase <= SKG_PHASE_DUST_EMISSION, "unknown phase");
+        REQUIRE(nell > 0 && ells, "no wavelengths given");
+        for (int i = 0; i < nell; i++) REQUIRE(ells[i] >= 0 && ells[i] < ctx->nlambda, "wavelength index out of range");
+        REQUIRE(count <= npp || npp == 0, "packet range exceeds the packet count");
+        if (phase != SKG_PHASE_STELLAR) REQUIRE(ctx->emit_cdf != nullptr, "dust phases need dust emission enabled");
+        cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+        if (nell > ctx->ells_cap) {
+            ctx->ells = ctx->A.alloc<int>(nell);
+            if (!ctx->ells) throw Failure{SKG_ERR_OOM, "device allocation failed"};
+            ctx->ells_cap = nell;
+        }
+        CK(cudaMemcpyAsync(ctx->ells, ells, nell * sizeof(int), cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(ctx->work, 0, sizeof(unsigned long long), s));
+        CK(cudaMemsetAsync(ctx->err, 0, sizeof(unsigned), s));
+        RunParams P;
+        std::memset(&P, 0, sizeof(P));
+        P.phase = phase; P.ells = ctx->ells; P.nell = nell;
+        P.npp = count; P.first_packet = first_packet; P.Npp_total = npp; P.seed = seed;
+        P.max_scatt = (opts && opts->max_scatt > 0) ? opts->max_scatt : 100000;
+        P.work = ctx->work; P.err = ctx->err; P.counters = ctx->counters;
+        DevGrid g = ctx->grid;
+        if (opts && opts->max_steps > 0) g.max_steps = opts->max_steps;
+        int precision = opts ? opts->precision : SKG_PREC_FP32;
+        int blocks = opts ? opts->blocks : 0, threads = opts ? opts->threads : 0;
+        if (count == 0) return SKG_OK;
+        CK(cudaEventRecord(ctx->ev0, s));
+        CK(launch_tracer(g, ctx->ds, P, precision, blocks, threads, s));
+        CK(cudaEventRecord(ctx->ev1, s));
+        return SKG_OK;
+    } catch (const Failure& f) { return fail(ctx, f); }
+}
+
+int skg_last_phase_ms(skg_ctx* ctx, float* ms) {
+    if (!ctx || !ms) return SKG_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaEventSynchronize(ctx->ev1);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, Failure{SKG_ERR_CUDA, cudaGetErrorString(e)}); }
+    cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
+    return SKG_OK;
+}
+
+int skg_reset_tallies(skg_ctx* ctx) {
+    if (!ctx) return SKG_ERR_INVALID;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t s = ctx->stream;
+        for (int i = 0; i < ctx->hs.ninstr; i++) {
+            if (ctx->cube_len[i]) CK(cudaMemsetAsync(ctx->hs.instr[i].cube, 0, ctx->cube_len[i] * sizeof(double), s));
+            CK(cudaMemsetAsync(ctx->hs.instr[i].sed, 0, ctx->sed_len[i] * sizeof(double), s));
+        }
+        size_t nlab = (size_t)ctx->ncells * ctx->nlambda;
+        if (ctx->hs.labs_stel) CK(cudaMemsetAsync(ctx->hs.labs_stel, 0, nlab * sizeof(double), s));
+        if (ctx->hs.labs_dust) CK(cudaMemsetAsync(ctx->hs.labs_dust, 0, nlab * sizeof(double), s));
+        CK(cudaMemsetAsync(ctx->counters, 0, 10 * sizeof(unsigned long long), s));
+        return SKG_OK;
+    } catch (const Failure& f) { return fail(ctx, f); }
+}
+
+int skg_tally_sizes(const skg_ctx* ctx, int instr, int64_t* cube_len, int64_t* sed_len) {
+    if (!ctx || instr < 0 || instr >= ctx->hs.ninstr) return SKG_ERR_INVALID;
+    if (cube_len) *cube_len = ctx->cube_len[instr];
+    if (sed_len) *sed_len = ctx->sed_len[instr];
+    return SKG_OK;
+}
+
+int skg_read_instrument(skg_ctx* ctx, int instr, double* cube, double* sed) {
+    if (!ctx || instr < 0 || instr >= ctx->hs.ninstr) return SKG_ERR_INVALID;
+    int rc = skg_sync(ctx, -1);
+    if (rc) return rc;
+    try {
+        if (cube && ctx->cube_len[instr])
+            CK(cudaMemcpy(cube, ctx->hs.instr[instr].cube, ctx->cube_len[instr] * sizeof(double), cudaMemcpyDeviceToHost));
+        if (sed) CK(cudaMemcpy(sed, ctx->hs.instr[instr].sed, ctx->sed_len[instr] * sizeof(double), cudaMemcpyDeviceToHost));
+        return SKG_OK;
+    } catch (const Failure& f) { return fail(ctx, f); }
+}
+
+int skg_read_absorption(skg_ctx* ctx, double* labs_stellar, double* labs_dust) {
+    if (!ctx) return SKG_ERR_INVALID;
+    int rc = skg_sync(ctx, -1);
+    if (rc) return rc;
+    try {
+        size_t n = (size_t)ctx->ncells * ctx->nlambda;
+        if (labs_stellar) {
+            if (ctx->hs.labs_stel) CK(cudaMemcpy(labs_stellar, ctx->hs.labs_stel, n * sizeof(double), cudaMemcpyDeviceToHost));
+            else std::memset(labs_stellar, 0, n * sizeof(double));
+        }
+        if (labs_dust) {
+            if (ctx->hs.labs_dust) CK(cudaMemcpy(labs_dust, ctx->hs.labs_dust, n * sizeof(double), cudaMemcpyDeviceToHost));
+            else std::memset(labs_dust, 0, n * sizeof(double));
+        }
+        return SKG_OK;
+    } catch (const Failure& f) { return fail(ctx, f); }
+}
+
+int skg_read_counters(skg_ctx* ctx, skg_counters* out) {
+    if (!ctx || !out) return SKG_ERR_INVALID;
+    int rc = skg_sync(ctx, -1);
+    if (rc && rc != SKG_ERR_STEP_BUDGET && rc != SKG_ERR_NAN_TAU) return rc;
+    unsigned long long c[10];
+    cudaMemcpy(c, ctx->counters, sizeof(c), cudaMemcpyDeviceToHost);
+    out->packets = c[0]; out->steps = c[1]; out->traversals = c[2]; out->scatterings = c[3]; out->peeloffs = c[4];
+    out->absorb_adds = c[5]; out->pixel_adds = c[6]; out->nbr_scanned = c[7]; out->fallbacks = c[8]; out->errors = c[9];
+    return rc;
+}
+
+int skg_calc_dust_emission(skg_ctx* ctx, double* temperature) {
+    if (!ctx) return SKG_ERR_INVALID;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        REQUIRE(ctx->emit_cdf != nullptr, "dust emission is not enabled for this scene");
+        cudaStream_t s = ctx->stream;
+        CK(launch_dust_emission(ctx->grid, ctx->ds, ctx->Tv, ctx->planckabs, ctx->nT, ctx->labsbol, ctx->spectra,
+                                ctx->temperature, s));
+        CK(launch_emission_sources(ctx->ds, ctx->nlambda, (int)ctx->ncells, ctx->labsbol, ctx->spectra, ctx->emit_Lv,
+                                   ctx->emit_cdf, ctx->emit_Ltot, ctx->scan_scratch, ctx->scan_bytes, s));
+        if (temperature) CK(cudaMemcpyAsync(temperature, ctx->temperature, ctx->ncells * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return SKG_OK;
+    } catch (const Failure& f) { return fail(ctx, f); }
+}
+
+int skg_absorbed_totals(skg_ctx* ctx, double* tot_stel, double* tot_dust) {
+    if (!ctx) return SKG_ERR_INVALID;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t s = ctx->stream;
+        size_t n = (size_t)ctx->ncells * ctx->nlambda;
+        double h[2] = {0, 0};
+        if (ctx->hs.labs_stel) CK(launch_sum(ctx->hs.labs_stel, n, ctx->sumbuf, s));
+        if (ctx->hs.labs_stel) CK(cudaMemcpyAsync(&h[0], ctx->sumbuf, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (ctx->hs.labs_dust) CK(launch_sum(ctx->hs.labs_dust, n, ctx->sumbuf + 1, s));
+        if (ctx->hs.labs_dust) CK(cudaMemcpyAsync(&h[1], ctx->sumbuf + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (tot_stel) *tot_stel = h[0];
+        if (tot_dust) *tot_dust = h[1];
+        return SKG_OK;
+    } catch (const Failure& f) { return fail(ctx, f); }
+}
+
+int skg_reset_dust_absorption(skg_ctx* ctx) {
+    if (!ctx) return SKG_ERR_INVALID;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        if (ctx->hs.labs_dust)
+            CK(cudaMemsetAsync(ctx->hs.labs_dust, 0, (size_t)ctx->ncells * ctx->nlambda * sizeof(double), ctx->stream));
+        return SKG_OK;
+    } catch (const Failure& f) { return fail(ctx, f); }
+}
+
+// ---------------------------------------------------------------------------------------------
+// trees
+
+int skg_tree_build(const skg_scene* sc, int type, int min_level, int max_level, double max_mass_fraction,
+                   int samples, uint64_t seed, int device, skg_tree** out) {
+    *out = nullptr;
+    skg_tree* T = new skg_tree();
+    try {
+        REQUIRE(sc && sc->ncomp > 0, "tree construction needs a dust distribution");
+        REQUIRE(type == SKG_GRID_OCTREE || type == SKG_GRID_BINTREE, "tree type must be octree or k-d tree");
+        REQUIRE(min_level >= 0 && max_level >= 2 && max_level > min_level && max_level <= 50, "invalid tree levels");
+        REQUIRE(samples >= 10 && samples <= 1000, "sample count must be in [10,1000]");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); throw Failure{SKG_ERR_NO_DEVICE, "no CUDA device"}; }
+        CK(cudaSetDevice(device));
+        cudaStream_t s;
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        Allocs A;
+        std::vector<DevGeometry> dg(sc->ncomp);
+        std::vector<double> norms(sc->ncomp);
+        double total_mass = 0;
+        for (int h = 0; h < sc->ncomp; h++) {
+            dg[h] = make_geometry(A, sc->dust[h].geometry, s);
+            norms[h] = sc->dust[h].norm; total_mass += norms[h];   // DustComp::mass() (DustComp.cpp:110-114)
+        }
+        DevGeometry* dgd = upload(A, dg.data(), dg.size(), s);
+        double* nd = upload(A, norms.data(), norms.size(), s);
+        Tree& t = T->t;
+        t.type = type;
+        t.ext[0] = sc->grid.xmin; t.ext[1] = sc->grid.ymin; t.ext[2] = sc->grid.zmin;
+        t.ext[3] = sc->grid.xmax; t.ext[4] = sc->grid.ymax; t.ext[5] = sc->grid.zmax;
+        Allocs B;
+        size_t cap = 0;
+        double *dbox = nullptr, *dm = nullptr, *dlo = nullptr, *dhi = nullptr;
+        auto sample = [&](const std::vector<int>& ids, std::vector<double>& mass, std::vector<double>& rmin,
+                          std::vector<double>& rmax) {
+            size_t n = ids.size();
+            if (n > cap) {
+                B.release();
+                cap = std::max(n, 2 * cap);
+                dbox = B.alloc<double>(6 * cap); dm = B.alloc<double>(cap); dlo = B.alloc<double>(cap); dhi = B.alloc<double>(cap);
+                if (!dbox || !dm || !dlo || !dhi) throw Failure{SKG_ERR_OOM, "device allocation failed"};
+            }
+            std::vector<double> hb(6 * n);
+            for (size_t q = 0; q < n; q++) std::memcpy(&hb[6 * q], t.nodes[ids[q]].box, 6 * sizeof(double));
+            CK(cudaMemcpyAsync(dbox, hb.data(), hb.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+            CK(launch_node_mass(dgd, nd, sc->ncomp, dbox, (int)n, samples, seed, (uint64_t)ids[0], dm, dlo, dhi, s));
+            mass.resize(n); rmin.resize(n); rmax.resize(n);
+            CK(cudaMemcpyAsync(mass.data(), dm, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(rmin.data(), dlo, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(rmax.data(), dhi, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+        };
+        t.build(min_level, max_level, max_mass_fraction, 0.0, 0.0, total_mass, sample);
+        CK(cudaStreamSynchronize(s));
+        cudaStreamDestroy(s);
+        t.finish(true);
+        t.flatten();
+        *out = T;
+        return SKG_OK;
+    } catch (const Failure& f) {
+        delete T;
+        return fail(nullptr, f);
+    }
+}
+
+int skg_tree_from_splits(int type, double xmin, double ymin, double zmin, double xmax, double ymax, double zmax,
+                         const uint8_t* split, int64_t nsplit, skg_tree** out) {
+    *out = nullptr;
+    if (type != SKG_GRID_OCTREE && type != SKG_GRID_BINTREE) { set_error("tree type must be octree or k-d tree"); return SKG_ERR_INVALID; }
+    skg_tree* T = new skg_tree();
+    Tree& t = T->t;
+    t.type = type;
+    t.ext[0] = xmin; t.ext[1] = ymin; t.ext[2] = zmin; t.ext[3] = xmax; t.ext[4] = ymax; t.ext[5] = zmax;
+    t.build_from_splits(split, nsplit);
+    t.finish(true);
+    t.flatten();
+    *out = T;
+    return SKG_OK;
+}
+
+int skg_tree_sizes(const skg_tree* T, int32_t* nnodes, int32_t* ncells, int64_t* nnbr) {
+    if (!T) return SKG_ERR_INVALID;
+    if (nnodes) *nnodes = (int32_t)T->t.nodes.size();
+    if (ncells) *ncells = T->t.ncells;
+    if (nnbr) *nnbr = (int64_t)T->t.nbr.size();
+    return SKG_OK;
+}
+
+int skg_tree_arrays(const skg_tree* T, double* node_box, int32_t* node_child, int32_t* node_father,
+                    int32_t* node_cell, int8_t* node_dir, int64_t* nbr_offsets, int32_t* nbr_ids) {
+    if (!T) return SKG_ERR_INVALID;
+    const Tree& t = T->t;
+    size_t n = t.nodes.size();
+    if (node_box) std::memcpy(node_box, t.box.data(), 6 * n * sizeof(double));
+    if (node_child) std::memcpy(node_child, t.child.data(), n * sizeof(int32_t));
+    if (node_father) std::memcpy(node_father, t.father.data(), n * sizeof(int32_t));
+    if (node_cell) std::memcpy(node_cell, t.cell.data(), n * sizeof(int32_t));
+    if (node_dir) std::memcpy(node_dir, t.dir.data(), n * sizeof(int8_t));
+    if (nbr_offsets) std::memcpy(nbr_offsets, t.nbroff.data(), t.nbroff.size() * sizeof(int64_t));
+    if (nbr_ids) std::memcpy(nbr_ids, t.nbr.data(), t.nbr.size() * sizeof(int32_t));
+    return SKG_OK;
+}
+
+int skg_tree_grid(const skg_tree* T, skg_grid* grid) {
+    if (!T || !grid) return SKG_ERR_INVALID;
+    T->t.fill_grid(grid);
+    return SKG_OK;
+}
+
+int skg_tree_destroy(skg_tree* T) { delete T; return SKG_OK; }
+
+}  // extern "C"

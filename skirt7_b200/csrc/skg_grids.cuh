@@ -1,0 +1,541 @@
+// skg_grids.cuh -- device views of the dust grids and their path steppers.
+//
+// A stepper produces the segments (cell m, length ds) of DustGrid::path one at a time, in the
+// order DustGridPath::addSegment receives them, without materialising the segment list.  The
+// FP64 instantiation repeats the reference's arithmetic operation for operation (compile its
+// users with --fmad=false for bit-identical cell sequences); the FP32 instantiation is the
+// production geometry.
+//   Cartesian : CartesianDustGrid::path   (SKIRTcore/CartesianDustGrid.cpp:136-283)
+//   Tree      : TreeDustGrid::path        (SKIRTcore/TreeDustGrid.cpp:371-643)
+//   Voronoi   : VoronoiMesh::path         (SKIRTcore/VoronoiMesh.cpp:778-873)
+#pragma once
+#include "skg_device.cuh"
+#include "../../include/skirt_b200.h"
+
+namespace skg {
+
+// Device view of a grid.  Both precisions are resident; kernels pick one by template.
+struct DevGrid {
+    int type;
+    double xmin, ymin, zmin, xmax, ymax, zmax;
+    double eps;                 // 1e-12 |diag| (TreeDustGrid.cpp:74, VoronoiMesh.cpp:220)
+    float  epsf;                // FP32 nudge (a few ulps of the domain size)
+    int ncells;
+    int max_steps;
+
+    // Cartesian planes
+    int nx, ny, nz;
+    const double *xv, *yv, *zv;
+    const float  *xvf, *yvf, *zvf;
+
+    // tree: node_box (6 doubles per node); nodef: 2 float4 per node
+    //   nodef[2l]   = (xmin, ymin, zmin, int child0 or -1)
+    //   nodef[2l+1] = (xmax, ymax, zmax, int cell or -1)
+    int nnodes;
+    const double* node_box;
+    const int*    node_child;
+    const int*    node_father;
+    const int*    node_cell;
+    const signed char* node_dir;
+    const float4* nodef;
+    const int*    nbroff;       // 6*nnodes+1
+    const int*    nbr;
+    const int*    cell_node;    // leaf node of each cell (TreeDustGrid::_idv)
+    int search;
+
+    // Voronoi: sites (3 doubles / float4), CSR neighbours, FP32 bisector planes per CSR entry
+    // vplane[q] = (n.x, n.y, n.z, n.p) with n = p_i - p_r and p the bisector midpoint; walls are
+    // encoded as axis planes, so s = (n.p - n.r)/(n.k) for every entry with n.k > 0.
+    int nsites;
+    const double* site;
+    const float4* sitef;
+    const int*    vnoff;
+    const int*    vnbr;
+    const float4* vplane;
+    int nb;
+    const int*    boff;
+    const int*    bids;
+    const double* vbbox;
+    const double* vvol;        // Voronoi cell volumes
+};
+
+// ---------------------------------------------------------------------------------------------
+// precision traits
+template<typename R> struct PT;
+template<> struct PT<double> {
+    static SKG_D double big() { return DBL_MAX; }
+    static SKG_D double eps(const DevGrid& g) { return g.eps; }
+};
+template<> struct PT<float> {
+    static SKG_D float big() { return FLT_MAX; }
+    static SKG_D float eps(const DevGrid& g) { return g.epsf; }
+};
+
+template<typename R> SKG_D R gx(const DevGrid& g, int i);
+template<> SKG_D double gx<double>(const DevGrid& g, int i) { return g.xv[i]; }
+template<> SKG_D float  gx<float>(const DevGrid& g, int i) { return g.xvf[i]; }
+template<typename R> SKG_D R gy(const DevGrid& g, int i);
+template<> SKG_D double gy<double>(const DevGrid& g, int i) { return g.yv[i]; }
+template<> SKG_D float  gy<float>(const DevGrid& g, int i) { return g.yvf[i]; }
+template<typename R> SKG_D R gz(const DevGrid& g, int i);
+template<> SKG_D double gz<double>(const DevGrid& g, int i) { return g.zv[i]; }
+template<> SKG_D float  gz<float>(const DevGrid& g, int i) { return g.zvf[i]; }
+
+// NR::locate_clip over a plane array (Fundamentals/NR.hpp:145-151)
+template<typename R, R (*A)(const DevGrid&, int)>
+SKG_D int locate_clip_dev(const DevGrid& g, int n /* planes */, R x) {
+    if (x < A(g, 0)) return 0;
+    int jl = -1, ju = n - 1;
+    while (ju - jl > 1) { int jm = (ju + jl) >> 1; if (x < A(g, jm)) ju = jm; else jl = jm; }
+    return jl;
+}
+
+// DustGridPath::moveInside (DustGridPath.cpp:57-150).  Returns false for OUTSIDE; entry
+// segments (m = -1) are appended to pend[] when their ds > 0.
+template<typename R>
+SKG_D bool move_inside(const DevGrid& g, R eps, R& rx, R& ry, R& rz, R kx, R ky, R kz,
+                       R* pend, int& npend) {
+    const R xmin = (R)g.xmin, xmax = (R)g.xmax, ymin = (R)g.ymin, ymax = (R)g.ymax,
+            zmin = (R)g.zmin, zmax = (R)g.zmax;
+    if (rx <= xmin) {
+        if (kx <= (R)0) return false;
+        R ds = (xmin - rx) / kx; if (ds > (R)0) pend[npend++] = ds;
+        rx = xmin + eps; ry += ky * ds; rz += kz * ds;
+    } else if (rx >= xmax) {
+        if (kx >= (R)0) return false;
+        R ds = (xmax - rx) / kx; if (ds > (R)0) pend[npend++] = ds;
+        rx = xmax - eps; ry += ky * ds; rz += kz * ds;
+    }
+    if (ry <= ymin) {
+        if (ky <= (R)0) return false;
+        R ds = (ymin - ry) / ky; if (ds > (R)0) pend[npend++] = ds;
+        rx += kx * ds; ry = ymin + eps; rz += kz * ds;
+    } else if (ry >= ymax) {
+        if (ky >= (R)0) return false;
+        R ds = (ymax - ry) / ky; if (ds > (R)0) pend[npend++] = ds;
+        rx += kx * ds; ry = ymax - eps; rz += kz * ds;
+    }
+    if (rz <= zmin) {
+        if (kz <= (R)0) return false;
+        R ds = (zmin - rz) / kz; if (ds > (R)0) pend[npend++] = ds;
+        rx += kx * ds; ry += ky * ds; rz = zmin + eps;
+    } else if (rz >= zmax) {
+        if (kz >= (R)0) return false;
+        R ds = (zmax - rz) / kz; if (ds > (R)0) pend[npend++] = ds;
+        rx += kx * ds; ry += ky * ds; rz = zmax - eps;
+    }
+    return true;
+}
+
+// =============================================================================================
+// Cartesian
+template<typename R>
+struct CartStepper {
+    R x, y, z, kx, ky, kz;
+    int i, j, k;
+    R pend[3]; int npend, ipend;
+    bool done;
+    int steps;
+    static constexpr int scanned = 0, fallbacks = 0;
+
+    SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz) {
+        x = rx; y = ry; z = rz; kx = dx; ky = dy; kz = dz;
+        npend = 0; ipend = 0; done = false; steps = 0;
+        const R xmin = (R)g.xmin, xmax = (R)g.xmax, ymin = (R)g.ymin, ymax = (R)g.ymax,
+                zmin = (R)g.zmin, zmax = (R)g.zmax;
+        R ds;
+        // entry into the box (CartesianDustGrid.cpp:151-222); "return path->clear()" empties the path
+        if (x < xmin) {
+            if (kx <= (R)0) { done = true; npend = 0; return; }
+            ds = (xmin - x) / kx; if (ds > (R)0) pend[npend++] = ds;
+            x = xmin + (R)1e-8 * (gx<R>(g, 1) - gx<R>(g, 0)); y += ky * ds; z += kz * ds;
+        } else if (x > xmax) {
+            if (kx >= (R)0) { done = true; npend = 0; return; }
+            ds = (xmax - x) / kx; if (ds > (R)0) pend[npend++] = ds;
+            x = xmax - (R)1e-8 * (gx<R>(g, g.nx) - gx<R>(g, g.nx - 1)); y += ky * ds; z += kz * ds;
+        }
+        if (y < ymin) {
+            if (ky <= (R)0) { done = true; npend = 0; return; }
+            ds = (ymin - y) / ky; if (ds > (R)0) pend[npend++] = ds;
+            x += kx * ds; y = ymin + (R)1e-8 * (gy<R>(g, 1) - gy<R>(g, 0)); z += kz * ds;
+        } else if (y > ymax) {
+            if (ky >= (R)0) { done = true; npend = 0; return; }
+            ds = (ymax - y) / ky; if (ds > (R)0) pend[npend++] = ds;
+            x += kx * ds; y = ymax - (R)1e-8 * (gy<R>(g, g.ny) - gy<R>(g, g.ny - 1)); z += kz * ds;
+        }
+        if (z < zmin) {
+            if (kz <= (R)0) { done = true; npend = 0; return; }
+            ds = (zmin - z) / kz; if (ds > (R)0) pend[npend++] = ds;
+            x += kx * ds; y += ky * ds; z = zmin + (R)1e-8 * (gz<R>(g, 1) - gz<R>(g, 0));
+        } else if (z > zmax) {
+            if (kz >= (R)0) { done = true; npend = 0; return; }
+            ds = (zmax - z) / kz; if (ds > (R)0) pend[npend++] = ds;
+            x += kx * ds; y += ky * ds; z = zmax - (R)1e-8 * (gz<R>(g, g.nz) - gz<R>(g, g.nz - 1));
+        }
+        if (x < xmin || x > xmax || y < ymin || y > ymax || z < zmin || z > zmax) { done = true; npend = 0; return; }
+        i = locate_clip_dev<R, gx<R>>(g, g.nx + 1, x);
+        j = locate_clip_dev<R, gy<R>>(g, g.ny + 1, y);
+        k = locate_clip_dev<R, gz<R>>(g, g.nz + 1, z);
+    }
+
+    // next segment; false when the path has ended
+    SKG_D bool next(const DevGrid& g, int& m, R& ds) {
+        if (ipend < npend) { m = -1; ds = pend[ipend++]; return true; }
+        while (!done) {
+            if (++steps > g.max_steps) { done = true; return false; }
+            m = k + g.nz * j + g.nz * g.ny * i;
+            R xE = (kx < (R)0) ? gx<R>(g, i) : gx<R>(g, i + 1);
+            R yE = (ky < (R)0) ? gy<R>(g, j) : gy<R>(g, j + 1);
+            R zE = (kz < (R)0) ? gz<R>(g, k) : gz<R>(g, k + 1);
+            R dsx = (fabs(kx) > (R)1e-15) ? (xE - x) / kx : PT<R>::big();
+            R dsy = (fabs(ky) > (R)1e-15) ? (yE - y) / ky : PT<R>::big();
+            R dsz = (fabs(kz) > (R)1e-15) ? (zE - z) / kz : PT<R>::big();
+            R d;
+            if (dsx <= dsy && dsx <= dsz) {
+                d = dsx;
+                i += (kx < (R)0) ? -1 : 1;
+                if (i >= g.nx || i < 0) done = true;
+                else { x = xE; y += ky * d; z += kz * d; }
+            } else if (dsy < dsx && dsy <= dsz) {
+                d = dsy;
+                j += (ky < (R)0) ? -1 : 1;
+                if (j >= g.ny || j < 0) done = true;
+                else { x += kx * d; y = yE; z += kz * d; }
+            } else if (dsz < dsx && dsz < dsy) {
+                d = dsz;
+                k += (kz < (R)0) ? -1 : 1;
+                if (k >= g.nz || k < 0) done = true;
+                else { x += kx * d; y += ky * d; z = zE; }
+            } else { done = true; return false; }   // NaN direction
+            if (d > (R)0) { ds = d; return true; }      // DustGridPath::addSegment drops ds <= 0
+        }
+        return false;
+    }
+};
+
+// =============================================================================================
+// Tree (octree and k-d tree)
+template<typename R> SKG_D void node_bounds(const DevGrid& g, int l, V3<R>& lo, V3<R>& hi);
+template<> SKG_D void node_bounds<double>(const DevGrid& g, int l, V3<double>& lo, V3<double>& hi) {
+    const double* b = g.node_box + 6 * (size_t)l;
+    lo = mk3(b[0], b[1], b[2]); hi = mk3(b[3], b[4], b[5]);
+}
+template<> SKG_D void node_bounds<float>(const DevGrid& g, int l, V3<float>& lo, V3<float>& hi) {
+    float4 a = __ldg(g.nodef + 2 * (size_t)l), b = __ldg(g.nodef + 2 * (size_t)l + 1);
+    lo = mk3(a.x, a.y, a.z); hi = mk3(b.x, b.y, b.z);
+}
+template<typename R> SKG_D V3<R> node_hi(const DevGrid& g, int l);
+template<> SKG_D V3<double> node_hi<double>(const DevGrid& g, int l) {
+    const double* b = g.node_box + 6 * (size_t)l; return mk3(b[3], b[4], b[5]);
+}
+template<> SKG_D V3<float> node_hi<float>(const DevGrid& g, int l) {
+    float4 b = __ldg(g.nodef + 2 * (size_t)l + 1); return mk3(b.x, b.y, b.z);
+}
+template<typename R> SKG_D bool box_contains(V3<R> lo, V3<R> hi, R x, R y, R z) {   // Box.hpp:80-81
+    return x >= lo.x && x <= hi.x && y >= lo.y && y <= hi.y && z >= lo.z && z <= hi.z;
+}
+
+// TreeNode::child(r): OctTreeNode.cpp:184-189 / BinTreeNode.cpp:326-335
+template<typename R>
+SKG_D int tree_child(const DevGrid& g, int l, R x, R y, R z) {
+    int c0 = g.node_child[l];
+    V3<R> s = node_hi<R>(g, c0);
+    int d = g.node_dir[l];
+    if (d < 0) return c0 + (x < s.x ? 0 : 1) + (y < s.y ? 0 : 2) + (z < s.z ? 0 : 4);
+    if (d == 0) return x < s.x ? c0 : c0 + 1;
+    if (d == 1) return y < s.y ? c0 : c0 + 1;
+    return z < s.z ? c0 : c0 + 1;
+}
+// TreeNode::whichnode from the root (TreeNode.cpp:70-80)
+template<typename R>
+SKG_D int tree_whichnode(const DevGrid& g, R x, R y, R z) {
+    V3<R> lo, hi; node_bounds<R>(g, 0, lo, hi);
+    if (!box_contains(lo, hi, x, y, z)) return -1;
+    int l = 0;
+    int guard = 0;
+    while (g.node_child[l] >= 0 && guard++ < 64) l = tree_child<R>(g, l, x, y, z);
+    return l;
+}
+
+template<typename R>
+struct TreeStepper {
+    R x, y, z, kx, ky, kz;
+    int node;
+    R pend[3]; int npend, ipend;
+    bool done;
+    int steps;
+    int fallbacks;
+    int scanned;
+
+    SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz) {
+        kx = dx; ky = dy; kz = dz; npend = 0; ipend = 0; done = false; steps = 0; fallbacks = 0; scanned = 0;
+        R eps = PT<R>::eps(g);
+        bool ok = move_inside<R>(g, eps, rx, ry, rz, kx, ky, kz, pend, npend);
+        node = ok ? tree_whichnode<R>(g, rx, ry, rz) : -1;
+        if (node < 0) { npend = 0; done = true; return; }   // path->clear()
+        x = rx; y = ry; z = rz;
+    }
+
+    SKG_D bool next(const DevGrid& g, int& m, R& ds) {
+        if (ipend < npend) { m = -1; ds = pend[ipend++]; return true; }
+        while (!done) {
+            if (++steps > g.max_steps) { done = true; return false; }
+            if (g.search == 2) { if (bookkeeping(g, m, ds)) return true; else continue; }
+            V3<R> lo, hi; node_bounds<R>(g, node, lo, hi);
+            R xnext = (kx < (R)0) ? lo.x : hi.x;
+            R ynext = (ky < (R)0) ? lo.y : hi.y;
+            R znext = (kz < (R)0) ? lo.z : hi.z;
+            R dsx = (fabs(kx) > (R)1e-15) ? (xnext - x) / kx : PT<R>::big();
+            R dsy = (fabs(ky) > (R)1e-15) ? (ynext - y) / ky : PT<R>::big();
+            R dsz = (fabs(kz) > (R)1e-15) ? (znext - z) / kz : PT<R>::big();
+            R d; int wall;
+            if (dsx <= dsy && dsx <= dsz) { d = dsx; wall = (kx < (R)0) ? 0 : 1; }
+            else if (dsy <= dsx && dsy <= dsz) { d = dsy; wall = (ky < (R)0) ? 2 : 3; }
+            else { d = dsz; wall = (kz < (R)0) ? 4 : 5; }
+            m = g.node_cell[node];
+            R eps = PT<R>::eps(g);
+            x += (d + eps) * kx; y += (d + eps) * ky; z += (d + eps) * kz;
+            int oldnode = node;
+            if (g.search == 1) {
+                int found = -1;
+                int q1 = g.nbroff[6 * node + wall + 1];
+                for (int q = g.nbroff[6 * node + wall]; q < q1; q++) {
+                    int c = __ldg(g.nbr + q);
+                    scanned++;
+                    V3<R> l2, h2; node_bounds<R>(g, c, l2, h2);
+                    if (box_contains(l2, h2, x, y, z)) { found = c; break; }
+                }
+                if (found < 0) { found = tree_whichnode<R>(g, x, y, z); fallbacks++; }
+                node = found;
+            } else {
+                node = tree_whichnode<R>(g, x, y, z);
+            }
+            if (node == oldnode) {      // TreeDustGrid.cpp:418-435
+                x = nextafter(x, (kx < (R)0) ? -PT<R>::big() : PT<R>::big());
+                y = nextafter(y, (ky < (R)0) ? -PT<R>::big() : PT<R>::big());
+                z = nextafter(z, (kz < (R)0) ? -PT<R>::big() : PT<R>::big());
+                node = tree_whichnode<R>(g, x, y, z);
+                if (node == oldnode) node = -1;
+            }
+            if (node < 0) done = true;
+            // FP32: the nudge past the wall is credited to this segment so that the total path
+            // length stays exact (FP64 keeps the reference's accounting)
+            if (sizeof(R) == 4 && node >= 0) d += eps;
+            if (d > (R)0) { ds = d; return true; }
+        }
+        return false;
+    }
+
+    // Bookkeeping search (TreeDustGrid.cpp:500-640), octree only: neighbour found by index
+    // arithmetic over siblings and fathers.  Returns true when a segment was produced.
+    SKG_D bool bookkeeping(const DevGrid& g, int& m, R& ds) {
+        int l = node;
+        V3<R> lo, hi; node_bounds<R>(g, l, lo, hi);
+        R xnext = (kx < (R)0) ? lo.x : hi.x;
+        R ynext = (ky < (R)0) ? lo.y : hi.y;
+        R znext = (kz < (R)0) ? lo.z : hi.z;
+        R dsx = (fabs(kx) > (R)1e-15) ? (xnext - x) / kx : PT<R>::big();
+        R dsy = (fabs(ky) > (R)1e-15) ? (ynext - y) / ky : PT<R>::big();
+        R dsz = (fabs(kz) > (R)1e-15) ? (znext - z) / kz : PT<R>::big();
+        R d;
+        m = g.node_cell[l];
+        if (dsx <= dsy && dsx <= dsz) {
+            d = dsx; x = xnext; y += ky * d; z += kz * d;
+            while (true) {
+                int oct = ((l - 1) % 8) + 1;
+                bool place = (kx < (R)0) ? (oct % 2 == 1) : (oct % 2 == 0);
+                if (!place) break;
+                l = g.node_father[l];
+                if (l == 0) { done = true; break; }
+            }
+            if (!done) {
+                l += (kx < (R)0) ? -1 : 1;
+                while (g.node_cell[l] == -1) {
+                    int c0 = g.node_child[l]; V3<R> s = node_hi<R>(g, c0);
+                    if (kx < (R)0) l = (y <= s.y) ? ((z <= s.z) ? c0 + 1 : c0 + 5) : ((z <= s.z) ? c0 + 3 : c0 + 7);
+                    else           l = (y <= s.y) ? ((z <= s.z) ? c0 + 0 : c0 + 4) : ((z <= s.z) ? c0 + 2 : c0 + 6);
+                }
+            }
+        } else if (dsy < dsx && dsy <= dsz) {
+            d = dsy; x += kx * d; y = ynext; z += kz * d;
+            while (true) {
+                bool place = (ky < (R)0) ? ((l - 1) % 4 < 2) : ((l - 1) % 4 > 1);
+                if (!place) break;
+                l = g.node_father[l];
+                if (l == 0) { done = true; break; }
+            }
+            if (!done) {
+                l += (ky < (R)0) ? -2 : 2;
+                while (g.node_cell[l] == -1) {
+                    int c0 = g.node_child[l]; V3<R> s = node_hi<R>(g, c0);
+                    if (ky < (R)0) l = (x <= s.x) ? ((z <= s.z) ? c0 + 2 : c0 + 6) : ((z <= s.z) ? c0 + 3 : c0 + 7);
+                    else           l = (x <= s.x) ? ((z <= s.z) ? c0 + 0 : c0 + 4) : ((z <= s.z) ? c0 + 1 : c0 + 5);
+                }
+            }
+        } else if (dsz < dsx && dsz < dsy) {
+            d = dsz; x += kx * d; y += ky * d; z = znext;
+            while (true) {
+                int oct = ((l - 1) % 8) + 1;
+                bool place = (kz < (R)0) ? (oct < 5) : (oct > 4);
+                if (!place) break;
+                l = g.node_father[l];
+                if (l == 0) { done = true; break; }
+            }
+            if (!done) {
+                l += (kz < (R)0) ? -4 : 4;
+                while (g.node_cell[l] == -1) {
+                    int c0 = g.node_child[l]; V3<R> s = node_hi<R>(g, c0);
+                    if (kz < (R)0) l = (x <= s.x) ? ((y <= s.y) ? c0 + 4 : c0 + 6) : ((y <= s.y) ? c0 + 5 : c0 + 7);
+                    else           l = (x <= s.x) ? ((y <= s.y) ? c0 + 0 : c0 + 2) : ((y <= s.y) ? c0 + 1 : c0 + 3);
+                }
+            }
+        } else { done = true; return false; }
+        node = l;
+        if (d > (R)0) { ds = d; return true; }
+        return false;
+    }
+};
+
+// =============================================================================================
+// Voronoi
+template<typename R> SKG_D V3<R> site_pos(const DevGrid& g, int m);
+template<> SKG_D V3<double> site_pos<double>(const DevGrid& g, int m) {
+    const double* p = g.site + 3 * (size_t)m; return mk3(p[0], p[1], p[2]);
+}
+template<> SKG_D V3<float> site_pos<float>(const DevGrid& g, int m) {
+    float4 p = __ldg(g.sitef + m); return mk3(p.x, p.y, p.z);
+}
+
+// VoronoiMesh::cellIndex (VoronoiMesh.cpp:541-570): nearest site among the cells overlapping the
+// block of the point (the reference's per-block kd-tree is an exact nearest search).
+template<typename R>
+SKG_D int voronoi_cell_index(const DevGrid& g, R x, R y, R z) {
+    if (!(x >= (R)g.xmin && x <= (R)g.xmax && y >= (R)g.ymin && y <= (R)g.ymax &&
+          z >= (R)g.zmin && z <= (R)g.zmax)) return -1;
+    int nb = g.nb;
+    // Box::cellindices (Box.hpp:120-125) evaluated in double
+    int i = max(0, min(nb - 1, (int)(nb * ((double)x - g.xmin) / (g.xmax - g.xmin))));
+    int j = max(0, min(nb - 1, (int)(nb * ((double)y - g.ymin) / (g.ymax - g.ymin))));
+    int k = max(0, min(nb - 1, (int)(nb * ((double)z - g.zmin) / (g.zmax - g.zmin))));
+    int b = (i * nb + j) * nb + k;
+    int m = -1; R mdist = PT<R>::big();
+    int q1 = g.boff[b + 1];
+    for (int q = g.boff[b]; q < q1; q++) {
+        int id = __ldg(g.bids + q);
+        V3<R> p = site_pos<R>(g, id);
+        R dx = x - p.x, dy = y - p.y, dz = z - p.z;
+        R d = dx * dx + dy * dy + dz * dz;
+        if (d < mdist) { m = id; mdist = d; }
+    }
+    return m;
+}
+
+template<typename R>
+struct VoronoiStepper {
+    R x, y, z, kx, ky, kz;
+    int mr;
+    R pend[3]; int npend, ipend;
+    bool done;
+    int steps;
+    int fallbacks;
+    int scanned;
+
+    SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz) {
+        kx = dx; ky = dy; kz = dz; npend = 0; ipend = 0; done = false; steps = 0; fallbacks = 0; scanned = 0;
+        R eps = PT<R>::eps(g);
+        bool ok = move_inside<R>(g, eps, rx, ry, rz, kx, ky, kz, pend, npend);
+        if (!ok) { rx = ry = rz = (R)INFINITY; }
+        mr = voronoi_cell_index<R>(g, rx, ry, rz);
+        if (mr < 0) { npend = 0; done = true; return; }
+        x = rx; y = ry; z = rz;
+    }
+
+    SKG_D bool next(const DevGrid& g, int& m, R& ds);
+};
+
+// FP64: the reference arithmetic on the generator sites (VoronoiMesh.cpp:803-858)
+template<>
+SKG_D bool VoronoiStepper<double>::next(const DevGrid& g, int& m, double& ds) {
+    if (ipend < npend) { m = -1; ds = pend[ipend++]; return true; }
+    while (!done) {
+        if (++steps > g.max_steps) { done = true; return false; }
+        V3<double> pr = site_pos<double>(g, mr);
+        double sq = DBL_MAX;
+        int mq = -99;
+        int q1 = g.vnoff[mr + 1];
+        for (int q = g.vnoff[mr]; q < q1; q++) {
+            int mi = g.vnbr[q];
+            double si = 0;
+            scanned++;
+            if (mi >= 0) {
+                V3<double> pi = site_pos<double>(g, mi);
+                double nx = pi.x - pr.x, ny = pi.y - pr.y, nz = pi.z - pr.z;
+                double ndotk = nx * kx + ny * ky + nz * kz;
+                if (ndotk > 0) {
+                    double px = 0.5 * (pi.x + pr.x), py = 0.5 * (pi.y + pr.y), pz = 0.5 * (pi.z + pr.z);
+                    si = (nx * (px - x) + ny * (py - y) + nz * (pz - z)) / ndotk;
+                }
+            } else {
+                switch (mi) {
+                    case -1: si = (g.xmin - x) / kx; break;
+                    case -2: si = (g.xmax - x) / kx; break;
+                    case -3: si = (g.ymin - y) / ky; break;
+                    case -4: si = (g.ymax - y) / ky; break;
+                    case -5: si = (g.zmin - z) / kz; break;
+                    default: si = (g.zmax - z) / kz; break;
+                }
+            }
+            if (si > 0 && si < sq) { sq = si; mq = mi; }
+        }
+        if (mq == -99) {
+            x += kx * g.eps; y += ky * g.eps; z += kz * g.eps;
+            mr = voronoi_cell_index<double>(g, x, y, z);
+            fallbacks++;
+            if (mr < 0) done = true;
+            continue;
+        }
+        m = mr; ds = sq;
+        x += (sq + g.eps) * kx; y += (sq + g.eps) * ky; z += (sq + g.eps) * kz;
+        mr = mq;
+        if (mr < 0) done = true;
+        return true;
+    }
+    return false;
+}
+
+// FP32: precomputed bisector planes, one 16-byte load per neighbour entry
+template<>
+SKG_D bool VoronoiStepper<float>::next(const DevGrid& g, int& m, float& ds) {
+    if (ipend < npend) { m = -1; ds = pend[ipend++]; return true; }
+    while (!done) {
+        if (++steps > g.max_steps) { done = true; return false; }
+        float sq = FLT_MAX;
+        int qbest = -1;
+        int q0 = g.vnoff[mr], q1 = g.vnoff[mr + 1];
+        for (int q = q0; q < q1; q++) {
+            float4 pl = __ldg(g.vplane + q);
+            float ndotk = pl.x * kx + pl.y * ky + pl.z * kz;
+            scanned++;
+            if (ndotk > 0.f) {
+                float si = (pl.w - (pl.x * x + pl.y * y + pl.z * z)) / ndotk;
+                if (si > 0.f && si < sq) { sq = si; qbest = q; }
+            }
+        }
+        if (qbest < 0) {
+            x += kx * g.epsf; y += ky * g.epsf; z += kz * g.epsf;
+            mr = voronoi_cell_index<float>(g, x, y, z);
+            fallbacks++;
+            if (mr < 0) done = true;
+            continue;
+        }
+        m = mr;
+        x += (sq + g.epsf) * kx; y += (sq + g.epsf) * ky; z += (sq + g.epsf) * kz;
+        mr = __ldg(g.vnbr + qbest);
+        if (mr < 0) done = true;
+        ds = (mr >= 0) ? sq + g.epsf : sq;   // the nudge is credited to this segment (exact total length)
+        return true;
+    }
+    return false;
+}
+
+}  // namespace skg
