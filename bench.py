@@ -224,13 +224,22 @@ def main():
     Npp = npp_rank * world                      # the simulation's packets per wavelength
     first = rank * npp_rank
     prec = A.PREC_FP64 if args.precision == "fp64" else A.PREC_FP32
-    stream = torch.cuda.current_stream(local).cuda_stream
+    # a dedicated stream: the launches, the events and the collective all go on it
+    tstream = torch.cuda.Stream(device=local)
+    handle = tstream.cuda_stream
+    # per-rank frames handed to the all-reduce (Instrument::sumResults, Instrument.cpp:57-65)
+    red = [torch.zeros(nl * 512 * 512, dtype=torch.float64, device="cuda") for _ in range(3)] if dist else None
 
-    # frames on the device for the all-reduce (N>1): a torch buffer per instrument
     def step(seed):
-        ctx.reset_tallies()
-        ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=seed, precision=prec, stream=stream)
+        ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=seed, precision=prec, stream=handle)
+        if dist:
+            with torch.cuda.stream(tstream):
+                for i, t in enumerate(red):
+                    ctx.read_instrument_device(i, t.data_ptr(), None, handle)
+                    dist.all_reduce(t)
 
+    ctx.reset_tallies()
+    ctx.sync()
     for w in range(args.warmup):
         step(1000 + w)
     torch.cuda.synchronize()
@@ -243,18 +252,10 @@ def main():
     clocks = Clocks(local)
     clocks.start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    red = None
-    if dist:
-        red = [torch.zeros(int(np.prod((1, nl, 512, 512))), dtype=torch.float64, device="cuda") for _ in range(3)]
-    step_ms_kernel = []
     for s in range(args.steps):
-        ctx.reset_tallies()
-        ev[s][0].record()
-        ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=2000 + s, precision=prec, stream=stream)
-        if dist:
-            for t in red:
-                dist.all_reduce(t)
-        ev[s][1].record()
+        ev[s][0].record(tstream)
+        step(2000 + s)
+        ev[s][1].record(tstream)
     torch.cuda.synchronize()
     clk = clocks.stop()
     ms = [a.elapsed_time(b) for a, b in ev]
@@ -290,9 +291,16 @@ def main():
     t0 = time.perf_counter()
     for s in range(args.steps):
         ctx.reset_tallies()
-        ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=3000 + s, precision=prec)
-        for i in range(3):
-            ctx.read_instrument(i)
+        if dist:
+            ctx.sync()
+            step(3000 + s)
+            if rank == 0:
+                host = [t.cpu() for t in red]      # the reduced frames, device -> host
+            torch.cuda.synchronize()
+        else:
+            ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=3000 + s, precision=prec)
+            for i in range(3):
+                ctx.read_instrument(i)             # synchronises, then device -> host
     e2e_s = time.perf_counter() - t0
     if dist:
         t = torch.tensor([e2e_s], device="cuda")

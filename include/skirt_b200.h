@@ -285,6 +285,11 @@ int  skg_reset_tallies(skg_ctx* ctx);
    (SKG_FULL_NBASE + nscatt_levels).  SED instruments have no cube. */
 int  skg_tally_sizes(const skg_ctx* ctx, int instr, int64_t* cube_len, int64_t* sed_len);
 int  skg_read_instrument(skg_ctx* ctx, int instr, double* cube, double* sed);
+/* Device-to-device copy of instrument instr's tallies into caller-owned DEVICE buffers, enqueued
+   on `stream` (a cudaStream_t; NULL = the context stream) after the work already on it.  This is
+   how ranks hand their frames to a collective (the reference's Instrument::sumResults,
+   Instrument.cpp:57-65) without the tallies leaving the device. */
+int  skg_read_instrument_device(skg_ctx* ctx, int instr, double* d_cube, double* d_sed, void* stream);
 /* Absorbed luminosity [ncells][nlambda] (stellar and dust parts separately; either may be NULL). */
 int  skg_read_absorption(skg_ctx* ctx, double* labs_stellar, double* labs_dust);
 int  skg_read_counters(skg_ctx* ctx, skg_counters* out);
@@ -326,16 +331,17 @@ int  skg_tree_arrays(const skg_tree* t, double* node_box, int32_t* node_child, i
 int  skg_tree_grid(const skg_tree* t, skg_grid* grid);
 int  skg_tree_destroy(skg_tree* t);
 
-/* Builds the Voronoi tessellation of `nsites` points clipped to the extent of `grid`
-   (VoronoiMesh::buildMesh, VoronoiMesh.cpp:297-405): per-site neighbour lists with the
-   wall ids -1..-6, cell volumes, centroids and bounding boxes, and the nb^3 block lists.
-   Cells are computed on the device by clipping against nearby bisector planes. */
+/* Builds the Voronoi tessellation of `nsites` points clipped to the given extent
+   (VoronoiMesh::buildMesh, VoronoiMesh.cpp:297-405): sites outside the extent and sites within
+   1e-12 of the extent diagonal of another are dropped as the reference does; per kept site the
+   neighbour list with the wall ids -1..-6, the cell volume, centroid and bounding box, and the
+   nb^3 block lists.  Cells are computed on the device by clipping against nearby bisector planes. */
 typedef struct skg_voronoi skg_voronoi;
 int  skg_voronoi_build(const double* sites, int32_t nsites, double xmin, double ymin, double zmin,
                        double xmax, double ymax, double zmax, int device, skg_voronoi** out);
 int  skg_voronoi_sizes(const skg_voronoi* v, int32_t* nsites, int64_t* nnbr, int32_t* nb,
                        int64_t* nblockids);
-int  skg_voronoi_arrays(const skg_voronoi* v, int64_t* vnbr_offsets, int32_t* vnbr_ids,
+int  skg_voronoi_arrays(const skg_voronoi* v, double* sites, int64_t* vnbr_offsets, int32_t* vnbr_ids,
                         double* volume, double* centroid, double* bbox,
                         int64_t* block_offsets, int32_t* block_ids);
 int  skg_voronoi_grid(const skg_voronoi* v, skg_grid* grid);

@@ -322,7 +322,9 @@ struct CartesianGrid : Grid {
         int i = locate_clip(xv.data(), Nx+1, x);
         int j = locate_clip(yv.data(), Ny+1, y);
         int k = locate_clip(zv.data(), Nz+1, z);
+        long guard = 0;
         while (true) {
+            if (++guard > (1L << 22)) return;   // test guard
             int m = index(i, j, k);
             double xE = (kx < 0.0) ? xv[i] : xv[i+1];
             double yE = (ky < 0.0) ? yv[j] : yv[j+1];
@@ -403,8 +405,10 @@ struct TreeGrid : Grid {
         if (node < 0) return p.clear();
         double x = bfr.x, y = bfr.y, z = bfr.z;
         double kx = p.k.x, ky = p.k.y, kz = p.k.z;
+        long guard = 0;
         if (search == SKG_SEARCH_TOPDOWN || search == SKG_SEARCH_NEIGHBOR) {
             while (node >= 0) {
+                if (++guard > (1L << 22)) break;   // test guard
                 const Box& b = box[node];
                 double xnext = (kx < 0.0) ? b.xmin : b.xmax;
                 double ynext = (ky < 0.0) ? b.ymin : b.ymax;
@@ -436,6 +440,7 @@ struct TreeGrid : Grid {
         } else {                                             // Bookkeeping (:500-640), octree only
             int l = node;
             while (true) {
+                if (++guard > (1L << 22)) return;   // test guard
                 const Box& b = box[l];
                 double xnext = (kx < 0.0) ? b.xmin : b.xmax;
                 double ynext = (ky < 0.0) ? b.ymin : b.ymax;
@@ -550,8 +555,9 @@ struct VoronoiGrid : Grid {
         if (!p.moveInside(ext, eps, r)) r = Vec(INFINITY, INFINITY, INFINITY);
         int mr = cellIndex(r);
         if (mr < 0) return p.clear();
-        int guard = 0;
+        long guard = 0;
         while (mr >= 0) {
+            if (++guard > (1L << 22)) { if (fallbacks) (*fallbacks)++; break; }   // test guard
             Vec pr = sites[mr];
             double sq = DBL_MAX;
             const int NO_INDEX = -99;
@@ -584,7 +590,6 @@ struct VoronoiGrid : Grid {
                 r = r + k*eps;
                 mr = cellIndex(r);
                 if (fallbacks) (*fallbacks)++;
-                if (++guard > 1000000) break;
             } else {
                 p.addSegment(mr, sq);
                 r = r + (sq+eps)*k;

@@ -130,6 +130,7 @@ FUNCS = {
     "skg_reset_tallies": (C.c_int, [C.c_void_p]),
     "skg_tally_sizes": (C.c_int, [C.c_void_p, C.c_int, i64p, i64p]),
     "skg_read_instrument": (C.c_int, [C.c_void_p, C.c_int, dp, dp]),
+    "skg_read_instrument_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "skg_read_absorption": (C.c_int, [C.c_void_p, dp, dp]),
     "skg_read_counters": (C.c_int, [C.c_void_p, C.POINTER(Counters)]),
     "skg_sync": (C.c_int, [C.c_void_p, C.c_int]),
@@ -148,7 +149,7 @@ FUNCS = {
     "skg_voronoi_build": (C.c_int, [dp, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_int, C.POINTER(C.c_void_p)]),
     "skg_voronoi_sizes": (C.c_int, [C.c_void_p, i32p, i64p, i32p, i64p]),
-    "skg_voronoi_arrays": (C.c_int, [C.c_void_p, i64p, i32p, dp, dp, dp, i64p, i32p]),
+    "skg_voronoi_arrays": (C.c_int, [C.c_void_p, dp, i64p, i32p, dp, dp, dp, i64p, i32p]),
     "skg_voronoi_grid": (C.c_int, [C.c_void_p, C.POINTER(Grid)]),
     "skg_voronoi_destroy": (C.c_int, [C.c_void_p]),
 }

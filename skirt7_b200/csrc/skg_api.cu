@@ -176,6 +176,43 @@ DevGrid make_grid(Allocs& A, const skg_grid& g, cudaStream_t s) {
             G.nbroff = upload(A, off.data(), off.size(), s);
             G.nbr = upload(A, g.nbr_ids, (size_t)tot, s);
         }
+        // leaf records for the FP32 walk: box, neighbour block offset and packed per-wall counts;
+        // the neighbour lists are re-indexed by cell number and grouped by wall
+        {
+            std::vector<float4> lr(2 * (size_t)nc);
+            std::vector<int> lnboff(6 * (size_t)nc + 1, 0), lnbr;
+            lnbr.reserve(g.nbr_offsets ? (size_t)g.nbr_offsets[6 * (size_t)n] : 0);
+            for (int m = 0; m < nc; m++) {
+                int l = cn[m];
+                const double* b = g.node_box + 6 * (size_t)l;
+                int base = (int)lnbr.size();
+                unsigned packed = 0;
+                bool fits = true;
+                for (int w = 0; w < 6; w++) {
+                    lnboff[6 * (size_t)m + w] = (int)lnbr.size();
+                    int cnt = 0;
+                    if (g.nbr_offsets) {
+                        for (int64_t q = g.nbr_offsets[6 * (size_t)l + w]; q < g.nbr_offsets[6 * (size_t)l + w + 1]; q++) {
+                            int c = g.node_cell[g.nbr_ids[q]];
+                            if (c < 0) continue;      // only leaves are ever matched
+                            lnbr.push_back(c); cnt++;
+                        }
+                    }
+                    if (cnt > 31) fits = false;
+                    else packed |= (unsigned)cnt << (5 * w);
+                }
+                if (!fits) packed = 0xFFFFFFFFu;
+                REQUIRE(lnbr.size() < (1ull << 31), "too many leaf neighbour entries");
+                float4 a, c;
+                a.x = (float)b[0]; a.y = (float)b[1]; a.z = (float)b[2]; std::memcpy(&a.w, &base, 4);
+                c.x = (float)b[3]; c.y = (float)b[4]; c.z = (float)b[5]; std::memcpy(&c.w, &packed, 4);
+                lr[2 * (size_t)m] = a; lr[2 * (size_t)m + 1] = c;
+            }
+            lnboff[6 * (size_t)nc] = (int)lnbr.size();
+            G.leafrec = upload(A, lr.data(), lr.size(), s);
+            G.lnbr = upload(A, lnbr.data(), lnbr.size(), s);
+            G.lnboff = upload(A, lnboff.data(), lnboff.size(), s);
+        }
         REQUIRE(g.search_method != SKG_SEARCH_BOOKKEEPING || g.type == SKG_GRID_OCTREE,
                 "the bookkeeping search method requires an octree");
     } else if (g.type == SKG_GRID_VORONOI) {
@@ -205,6 +242,9 @@ DevGrid make_grid(Allocs& A, const skg_grid& g, cudaStream_t s) {
                     REQUIRE(mi < n, "Voronoi neighbour id out of range");
                     const double* pi = g.sites + 3 * (size_t)mi;
                     nx = pi[0] - pr[0]; ny = pi[1] - pr[1]; nz = pi[2] - pr[2];
+                    // unit normal: n.p with unnormalised n (~1e19 m x 1e20 m) overflows FP32
+                    double inv = 1.0 / std::sqrt(nx * nx + ny * ny + nz * nz);
+                    nx *= inv; ny *= inv; nz *= inv;
                     w = nx * 0.5 * (pi[0] + pr[0]) + ny * 0.5 * (pi[1] + pr[1]) + nz * 0.5 * (pi[2] + pr[2]);
                 } else {
                     nx = ny = nz = 0;
@@ -713,6 +753,20 @@ int skg_read_instrument(skg_ctx* ctx, int instr, double* cube, double* sed) {
         if (cube && ctx->cube_len[instr])
             CK(cudaMemcpy(cube, ctx->hs.instr[instr].cube, ctx->cube_len[instr] * sizeof(double), cudaMemcpyDeviceToHost));
         if (sed) CK(cudaMemcpy(sed, ctx->hs.instr[instr].sed, ctx->sed_len[instr] * sizeof(double), cudaMemcpyDeviceToHost));
+        return SKG_OK;
+    } catch (const Failure& f) { return fail(ctx, f); }
+}
+
+int skg_read_instrument_device(skg_ctx* ctx, int instr, double* d_cube, double* d_sed, void* stream) {
+    if (!ctx || instr < 0 || instr >= ctx->hs.ninstr) return SKG_ERR_INVALID;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+        if (d_cube && ctx->cube_len[instr])
+            CK(cudaMemcpyAsync(d_cube, ctx->hs.instr[instr].cube, ctx->cube_len[instr] * sizeof(double),
+                               cudaMemcpyDeviceToDevice, s));
+        if (d_sed) CK(cudaMemcpyAsync(d_sed, ctx->hs.instr[instr].sed, ctx->sed_len[instr] * sizeof(double),
+                                      cudaMemcpyDeviceToDevice, s));
         return SKG_OK;
     } catch (const Failure& f) { return fail(ctx, f); }
 }

@@ -42,6 +42,14 @@ struct DevGrid {
     const int*    nbr;
     const int*    cell_node;    // leaf node of each cell (TreeDustGrid::_idv)
     int search;
+    // FP32 walk: one 32-byte record per leaf, indexed by cell number,
+    //   leafrec[2m]   = (xmin, ymin, zmin, int offset of the leaf's neighbour block in lnbr)
+    //   leafrec[2m+1] = (xmax, ymax, zmax, uint per-wall neighbour counts, 5 bits each, or ~0u)
+    // lnbr holds neighbour CELL numbers grouped by wall; lnboff[6m+w] are the per-wall offsets
+    // (read only when a wall has more than 31 neighbours).
+    const float4* leafrec;
+    const int*    lnbr;
+    const int*    lnboff;
 
     // Voronoi: sites (3 doubles / float4), CSR neighbours, FP32 bisector planes per CSR entry
     // vplane[q] = (n.x, n.y, n.z, n.p) with n = p_i - p_r and p the bisector midpoint; walls are
@@ -136,13 +144,23 @@ struct CartStepper {
     R pend[3]; int npend, ipend;
     bool done;
     int steps;
+    int cell0;                  // cell holding the start position (-1 if it lies outside the grid)
     static constexpr int scanned = 0, fallbacks = 0;
 
-    SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz) {
+    // hint: a cell known to hold the start position (or -1); it is verified against the planes
+    SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz, int hint = -1) {
         x = rx; y = ry; z = rz; kx = dx; ky = dy; kz = dz;
-        npend = 0; ipend = 0; done = false; steps = 0;
+        npend = 0; ipend = 0; done = false; steps = 0; cell0 = -1;
         const R xmin = (R)g.xmin, xmax = (R)g.xmax, ymin = (R)g.ymin, ymax = (R)g.ymax,
                 zmin = (R)g.zmin, zmax = (R)g.zmax;
+        if (hint >= 0) {
+            int hi_ = hint / (g.nz * g.ny), hj = (hint / g.nz) % g.ny, hk = hint % g.nz;
+            if (x >= gx<R>(g, hi_) && x <= gx<R>(g, hi_ + 1) && y >= gy<R>(g, hj) && y <= gy<R>(g, hj + 1) &&
+                z >= gz<R>(g, hk) && z <= gz<R>(g, hk + 1)) {
+                i = hi_; j = hj; k = hk; cell0 = hint;
+                return;
+            }
+        }
         R ds;
         // entry into the box (CartesianDustGrid.cpp:151-222); "return path->clear()" empties the path
         if (x < xmin) {
@@ -176,6 +194,7 @@ struct CartStepper {
         i = locate_clip_dev<R, gx<R>>(g, g.nx + 1, x);
         j = locate_clip_dev<R, gy<R>>(g, g.ny + 1, y);
         k = locate_clip_dev<R, gz<R>>(g, g.nz + 1, z);
+        if (npend == 0) cell0 = k + g.nz * j + g.nz * g.ny * i;
     }
 
     // next segment; false when the path has ended
@@ -258,7 +277,7 @@ SKG_D int tree_whichnode(const DevGrid& g, R x, R y, R z) {
 }
 
 template<typename R>
-struct TreeStepper {
+struct TreeNodeWalk {
     R x, y, z, kx, ky, kz;
     int node;
     R pend[3]; int npend, ipend;
@@ -266,13 +285,21 @@ struct TreeStepper {
     int steps;
     int fallbacks;
     int scanned;
+    int cell0;
 
-    SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz) {
+    SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz, int hint = -1) {
         kx = dx; ky = dy; kz = dz; npend = 0; ipend = 0; done = false; steps = 0; fallbacks = 0; scanned = 0;
+        cell0 = -1;
+        if (hint >= 0) {
+            int l = g.cell_node[hint];
+            V3<R> lo, hi; node_bounds<R>(g, l, lo, hi);
+            if (box_contains(lo, hi, rx, ry, rz)) { node = l; x = rx; y = ry; z = rz; cell0 = hint; return; }
+        }
         R eps = PT<R>::eps(g);
         bool ok = move_inside<R>(g, eps, rx, ry, rz, kx, ky, kz, pend, npend);
         node = ok ? tree_whichnode<R>(g, rx, ry, rz) : -1;
         if (node < 0) { npend = 0; done = true; return; }   // path->clear()
+        if (npend == 0) cell0 = g.node_cell[node];
         x = rx; y = ry; z = rz;
     }
 
@@ -396,6 +423,115 @@ struct TreeStepper {
     }
 };
 
+// FP32 production walk of the tree with the Neighbor search (TreeDustGrid.cpp:443-497): the
+// current leaf's 32-byte record stays in registers, so a step costs two dependent loads -- the
+// neighbour ids of the exit wall and the candidate's record, which becomes the next current one.
+// TopDown and Bookkeeping run through the node-based walk above.
+template<typename R> struct TreeStepper : TreeNodeWalk<R> {};
+
+template<>
+struct TreeStepper<float> {
+    float x, y, z, kx, ky, kz;
+    int cell;
+    float4 lo, hi;
+    int node;                   // node-based walk (search methods other than Neighbor)
+    float pend[3]; int npend, ipend;
+    bool done;
+    int steps, fallbacks, scanned;
+    int cell0;
+    TreeNodeWalk<float> bk;     // Bookkeeping search (octree index arithmetic)
+
+    SKG_D void load(const DevGrid& g, int m) { lo = __ldg(g.leafrec + 2 * (size_t)m); hi = __ldg(g.leafrec + 2 * (size_t)m + 1); }
+    SKG_D static bool inbox(float4 a, float4 b, float px, float py, float pz) {
+        return px >= a.x && px <= b.x && py >= a.y && py <= b.y && pz >= a.z && pz <= b.z;
+    }
+    SKG_D int descend(const DevGrid& g, float px, float py, float pz) {
+        int l = tree_whichnode<float>(g, px, py, pz);
+        return l >= 0 ? g.node_cell[l] : -1;
+    }
+
+    SKG_D void init(const DevGrid& g, float rx, float ry, float rz, float dx, float dy, float dz, int hint = -1) {
+        kx = dx; ky = dy; kz = dz; npend = 0; ipend = 0; done = false; steps = 0; fallbacks = 0; scanned = 0;
+        cell0 = -1;
+        if (g.search == SKG_SEARCH_BOOKKEEPING) {
+            bk.init(g, rx, ry, rz, dx, dy, dz, hint);
+            cell0 = bk.cell0; done = bk.done;
+            return;
+        }
+        if (hint >= 0) {
+            load(g, hint);
+            if (inbox(lo, hi, rx, ry, rz)) { cell = hint; cell0 = hint; x = rx; y = ry; z = rz; return; }
+        }
+        bool ok = move_inside<float>(g, g.epsf, rx, ry, rz, kx, ky, kz, pend, npend);
+        cell = ok ? descend(g, rx, ry, rz) : -1;
+        if (cell < 0) { npend = 0; done = true; return; }
+        if (npend == 0) cell0 = cell;
+        load(g, cell);
+        x = rx; y = ry; z = rz;
+    }
+
+    SKG_D bool next(const DevGrid& g, int& m, float& ds) {
+        if (g.search == SKG_SEARCH_BOOKKEEPING) {
+            bool r = bk.next(g, m, ds);
+            steps = bk.steps; done = bk.done;
+            return r;
+        }
+        if (ipend < npend) { m = -1; ds = pend[ipend++]; return true; }
+        const float eps = g.epsf;
+        while (!done) {
+            if (++steps > g.max_steps) { done = true; return false; }
+            float xnext = (kx < 0.f) ? lo.x : hi.x;
+            float ynext = (ky < 0.f) ? lo.y : hi.y;
+            float znext = (kz < 0.f) ? lo.z : hi.z;
+            float dsx = (fabsf(kx) > 1e-15f) ? (xnext - x) / kx : FLT_MAX;
+            float dsy = (fabsf(ky) > 1e-15f) ? (ynext - y) / ky : FLT_MAX;
+            float dsz = (fabsf(kz) > 1e-15f) ? (znext - z) / kz : FLT_MAX;
+            float d; int wall;
+            if (dsx <= dsy && dsx <= dsz) { d = dsx; wall = (kx < 0.f) ? 0 : 1; }
+            else if (dsy <= dsx && dsy <= dsz) { d = dsy; wall = (ky < 0.f) ? 2 : 3; }
+            else { d = dsz; wall = (kz < 0.f) ? 4 : 5; }
+            m = cell;
+            x += (d + eps) * kx; y += (d + eps) * ky; z += (d + eps) * kz;
+            // neighbours across the exit wall (TreeNode::whichnode(wall, r), TreeNode.cpp:84-93)
+            unsigned packed = __float_as_uint(hi.w);
+            int base = __float_as_int(lo.w), q0, cnt;
+            if (packed != 0xFFFFFFFFu) {
+                int pre = 0;
+                for (int w = 0; w < wall; w++) pre += (packed >> (5 * w)) & 31u;
+                q0 = base + pre; cnt = (packed >> (5 * wall)) & 31u;
+            } else {
+                q0 = g.lnboff[6 * cell + wall]; cnt = g.lnboff[6 * cell + wall + 1] - q0;
+            }
+            int found = -1;
+            float4 nlo, nhi;
+            if (g.search == SKG_SEARCH_TOPDOWN) cnt = 0;   // TopDown: always from the root
+            for (int q = 0; q < cnt; q++) {
+                int c = __ldg(g.lnbr + q0 + q);
+                scanned++;
+                nlo = __ldg(g.leafrec + 2 * (size_t)c); nhi = __ldg(g.leafrec + 2 * (size_t)c + 1);
+                if (inbox(nlo, nhi, x, y, z)) { found = c; break; }
+            }
+            if (found < 0) {                       // rounding near a corner: search from the root
+                found = descend(g, x, y, z);
+                if (g.search != SKG_SEARCH_TOPDOWN) fallbacks++;
+                if (found >= 0) { nlo = __ldg(g.leafrec + 2 * (size_t)found); nhi = __ldg(g.leafrec + 2 * (size_t)found + 1); }
+            }
+            if (found == cell) {                   // stuck (TreeDustGrid.cpp:476-493)
+                x = nextafterf(x, (kx < 0.f) ? -FLT_MAX : FLT_MAX);
+                y = nextafterf(y, (ky < 0.f) ? -FLT_MAX : FLT_MAX);
+                z = nextafterf(z, (kz < 0.f) ? -FLT_MAX : FLT_MAX);
+                found = descend(g, x, y, z);
+                if (found == cell) found = -1;
+                else if (found >= 0) { nlo = __ldg(g.leafrec + 2 * (size_t)found); nhi = __ldg(g.leafrec + 2 * (size_t)found + 1); }
+            }
+            if (found < 0) done = true;
+            else { cell = found; lo = nlo; hi = nhi; d += eps; }   // the nudge is credited to this segment
+            if (d > 0.f) { ds = d; return true; }
+        }
+        return false;
+    }
+};
+
 // =============================================================================================
 // Voronoi
 template<typename R> SKG_D V3<R> site_pos(const DevGrid& g, int m);
@@ -418,13 +554,14 @@ SKG_D int voronoi_cell_index(const DevGrid& g, R x, R y, R z) {
     int j = max(0, min(nb - 1, (int)(nb * ((double)y - g.ymin) / (g.ymax - g.ymin))));
     int k = max(0, min(nb - 1, (int)(nb * ((double)z - g.zmin) / (g.zmax - g.zmin))));
     int b = (i * nb + j) * nb + k;
-    int m = -1; R mdist = PT<R>::big();
+    // squared distances in FP64 for both precisions (they overflow FP32 for galaxy-sized domains)
+    int m = -1; double mdist = DBL_MAX;
     int q1 = g.boff[b + 1];
     for (int q = g.boff[b]; q < q1; q++) {
         int id = __ldg(g.bids + q);
-        V3<R> p = site_pos<R>(g, id);
-        R dx = x - p.x, dy = y - p.y, dz = z - p.z;
-        R d = dx * dx + dy * dy + dz * dz;
+        V3<double> p = site_pos<double>(g, id);
+        double dx = (double)x - p.x, dy = (double)y - p.y, dz = (double)z - p.z;
+        double d = dx * dx + dy * dy + dz * dz;
         if (d < mdist) { m = id; mdist = d; }
     }
     return m;
@@ -439,14 +576,24 @@ struct VoronoiStepper {
     int steps;
     int fallbacks;
     int scanned;
+    int cell0;
 
-    SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz) {
+    // hint: the cell holding the start position (the interaction point lies in the cell of its
+    // segment); accepted for a position strictly inside the domain
+    SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz, int hint = -1) {
         kx = dx; ky = dy; kz = dz; npend = 0; ipend = 0; done = false; steps = 0; fallbacks = 0; scanned = 0;
+        cell0 = -1;
+        if (hint >= 0 && rx > (R)g.xmin && rx < (R)g.xmax && ry > (R)g.ymin && ry < (R)g.ymax &&
+            rz > (R)g.zmin && rz < (R)g.zmax) {
+            mr = hint; cell0 = hint; x = rx; y = ry; z = rz;
+            return;
+        }
         R eps = PT<R>::eps(g);
         bool ok = move_inside<R>(g, eps, rx, ry, rz, kx, ky, kz, pend, npend);
         if (!ok) { rx = ry = rz = (R)INFINITY; }
         mr = voronoi_cell_index<R>(g, rx, ry, rz);
         if (mr < 0) { npend = 0; done = true; return; }
+        if (npend == 0) cell0 = mr;
         x = rx; y = ry; z = rz;
     }
 

@@ -107,6 +107,7 @@ tracer_kernel(const DevGrid g, const DevScene* __restrict__ Sp, const RunParams 
     V3<R> r = mk3((R)0, (R)0, (R)0), k = mk3((R)0, (R)0, (R)1);
     int mode = M_FETCH, trav = T_NONE;
     int int_cell = -1;
+    int pos_cell = -2;          // cell holding the packet position: -2 unknown, -1 outside the grid
     double tau = 0, s = 0, tau_int = 0, s_int = 0;
     Stepper<R> st;
     unsigned c_steps = 0, c_trav = 0, c_scatt = 0, c_peel = 0, c_abs = 0, c_pix = 0, c_nbr = 0, c_fb = 0,
@@ -129,6 +130,7 @@ tracer_kernel(const DevGrid g, const DevScene* __restrict__ Sp, const RunParams 
                 ell = P.ells[ei];
                 rng.init(P.seed, P.first_packet + ip, (uint32_t)ell | ((uint32_t)P.phase << 24));
                 c_pk++;
+                pos_cell = -2;
                 nscatt = 0;
                 V3<double> pos, dir;
                 if (!dust_phase) {
@@ -206,7 +208,8 @@ tracer_kernel(const DevGrid g, const DevScene* __restrict__ Sp, const RunParams 
                     }
                     Lpeel = L * w;
                     if (group_needs_traversal(S, grp, (double)r.x, (double)r.y, (double)r.z)) {
-                        st.init(g, r.x, r.y, r.z, (R)S.gkx[grp], (R)S.gky[grp], (R)S.gkz[grp]);
+                        st.init(g, r.x, r.y, r.z, (R)S.gkx[grp], (R)S.gky[grp], (R)S.gkz[grp], pos_cell);
+                        if (pos_cell == -2) pos_cell = st.cell0;
                         trav = T_PEEL; tau = 0;
                         break;
                     }
@@ -217,7 +220,8 @@ tracer_kernel(const DevGrid g, const DevScene* __restrict__ Sp, const RunParams 
             }
             case M_MAIN1_START: {
                 if (S.ncomp == 0) { mode = M_FETCH; break; }
-                st.init(g, r.x, r.y, r.z, k.x, k.y, k.z);
+                st.init(g, r.x, r.y, r.z, k.x, k.y, k.z, pos_cell);
+                if (pos_cell == -2) pos_cell = st.cell0;
                 trav = T_MAIN1; tau = 0; Lsca_acc = 0;
                 break;
             }
@@ -249,13 +253,15 @@ tracer_kernel(const DevGrid g, const DevScene* __restrict__ Sp, const RunParams 
                     L *= p / q;
                 }
                 tau_int = ti;
-                st.init(g, r.x, r.y, r.z, k.x, k.y, k.z);
+                st.init(g, r.x, r.y, r.z, k.x, k.y, k.z, pos_cell);
                 trav = T_MAIN2; tau = 0; s = 0; s_int = -1; int_cell = -1;
                 break;
             }
             case M_AFTER_MAIN2: {
                 R si = (R)s_int;
                 r = mk3(r.x + si * k.x, r.y + si * k.y, r.z + si * k.z);   // PhotonPackage::propagate
+                // the interaction point lies in the cell of its segment (verified by the stepper)
+                if (s_int > 0) pos_cell = (int_cell >= 0) ? int_cell : -2;
                 if (peel_on) { mode = M_PEEL_NEXT; grp = 0; scat_peel = true; }
                 else mode = M_SCATTER;
                 break;

@@ -118,6 +118,11 @@ class Context:
             cube = cube.reshape(ncomp, self.nlambda, ins.pixelsY, ins.pixelsX)
         return cube, sed
 
+    def read_instrument_device(self, i, d_cube, d_sed=None, stream=None):
+        """Copies instrument i's tallies into caller-owned device buffers (raw device pointers,
+        e.g. torch tensor data_ptr()) on the given stream."""
+        self._ck(self.lib.skg_read_instrument_device(self.h, i, d_cube, d_sed, stream))
+
     def read_absorption(self):
         ls = np.zeros(self.ncells * self.nlambda)
         ld = np.zeros(self.ncells * self.nlambda)

@@ -82,9 +82,10 @@ def test_stellar_phase_matches_oracle(orc, precision):
         fc = lambda r, c=c: block_sum(r["inst"][2][0][c, 0], 6)
         z, ok = _well_sampled(zscores([fc(g) for g in G], [fc(o) for o in O]), O, fc)
         _check(z, ok, "full frame component %d" % c)
-    # SimpleInstrument shares the 88-degree direction group with the frame: identical frames
+    # SimpleInstrument shares the 88-degree direction group with the frame: the same frame up to
+    # the summation order of the FP64 atomics
     for g in G:
-        assert np.allclose(g["inst"][3][0][0, 0], g["inst"][0][0][0, 0], rtol=0, atol=0)
+        assert np.allclose(g["inst"][3][0][0, 0], g["inst"][0][0][0, 0], rtol=1e-12, atol=0)
     # absorbed luminosity per cell, summed over slabs of constant x index (40 slabs)
     nx = 40
     fl = lambda r: r["labs"].reshape(nx, -1).sum(1)
