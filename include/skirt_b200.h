@@ -276,6 +276,34 @@ int  skg_run_phase(skg_ctx* ctx, int phase, const int32_t* ells, int nell, uint6
                    uint64_t first_packet, uint64_t count, uint64_t seed, const skg_run_opts* opts,
                    void* stream);
 
+/* ---- batched launches (many simulations in one persistent launch) ------------------------ */
+/* A slice of one simulation: packets [first, first+count) of each listed wavelength, each carrying
+   L/npp of the simulation. */
+typedef struct skg_work {
+    skg_ctx* ctx;
+    const int32_t* ells;
+    int32_t nell;
+    uint64_t npp, first, count, seed;
+} skg_work;
+typedef struct skg_batch skg_batch;
+/* Staging for batched launches on one device: up to max_slots distinct simulations, max_items
+   slices and max_ells wavelength entries per launch. */
+int  skg_batch_create(int device, int max_slots, int max_items, int max_ells, skg_batch** out);
+int  skg_batch_destroy(skg_batch* b);
+/* Runs the slices in ONE persistent launch (all contexts on the batch's device, same grid type).
+   A packet's random stream depends only on (seed, packet id, wavelength, phase), so a
+   simulation's tallies are the same alone and mixed with others, up to the summation order of the
+   FP64 atomics.  With SKG_BATCH_GRAPH in `flags` the launch sequence (table uploads, counter
+   reset, tracer) is captured once into a CUDA graph and replayed while the grid type and launch
+   configuration stay the same.  Returns once enqueued on `stream` (NULL = the batch's own
+   stream). */
+#define SKG_BATCH_GRAPH 1
+int  skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, const skg_run_opts* opts,
+                   int flags, void* stream);
+int  skg_batch_sync(skg_batch* b, int timeout_ms);
+int  skg_batch_counters(skg_batch* b, skg_counters* out);
+int  skg_batch_last_ms(skg_batch* b, float* ms);
+
 /* Zeroes all tallies (instrument cubes and SEDs, absorbed luminosity). */
 int  skg_reset_tallies(skg_ctx* ctx);
 

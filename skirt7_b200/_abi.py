@@ -112,6 +112,13 @@ class Counters(C.Structure):
         "nbr_scanned", "fallbacks", "errors")]
 
 
+class Work(C.Structure):
+    _fields_ = [("ctx", C.c_void_p), ("ells", i32p), ("nell", C.c_int32), ("npp", C.c_uint64), ("first", C.c_uint64),
+                ("count", C.c_uint64), ("seed", C.c_uint64)]
+
+
+BATCH_GRAPH = 1
+
 # exported functions: name -> (restype, argtypes)
 FUNCS = {
     "skg_version": (C.c_int, []),
@@ -128,6 +135,13 @@ FUNCS = {
     "skg_run_phase": (C.c_int, [C.c_void_p, C.c_int, i32p, C.c_int, C.c_uint64, C.c_uint64, C.c_uint64,
                                 C.c_uint64, C.POINTER(RunOpts), C.c_void_p]),
     "skg_reset_tallies": (C.c_int, [C.c_void_p]),
+    "skg_batch_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "skg_batch_destroy": (C.c_int, [C.c_void_p]),
+    "skg_batch_run": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Work), C.c_int, C.POINTER(RunOpts), C.c_int,
+                                C.c_void_p]),
+    "skg_batch_sync": (C.c_int, [C.c_void_p, C.c_int]),
+    "skg_batch_counters": (C.c_int, [C.c_void_p, C.POINTER(Counters)]),
+    "skg_batch_last_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "skg_tally_sizes": (C.c_int, [C.c_void_p, C.c_int, i64p, i64p]),
     "skg_read_instrument": (C.c_int, [C.c_void_p, C.c_int, dp, dp]),
     "skg_read_instrument_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),

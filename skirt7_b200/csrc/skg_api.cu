@@ -176,42 +176,14 @@ DevGrid make_grid(Allocs& A, const skg_grid& g, cudaStream_t s) {
             G.nbroff = upload(A, off.data(), off.size(), s);
             G.nbr = upload(A, g.nbr_ids, (size_t)tot, s);
         }
-        // leaf records for the FP32 walk: box, neighbour block offset and packed per-wall counts;
-        // the neighbour lists are re-indexed by cell number and grouped by wall
+        // rope-linked tree for the FP32 walk
         {
-            std::vector<float4> lr(2 * (size_t)nc);
-            std::vector<int> lnboff(6 * (size_t)nc + 1, 0), lnbr;
-            lnbr.reserve(g.nbr_offsets ? (size_t)g.nbr_offsets[6 * (size_t)n] : 0);
-            for (int m = 0; m < nc; m++) {
-                int l = cn[m];
-                const double* b = g.node_box + 6 * (size_t)l;
-                int base = (int)lnbr.size();
-                unsigned packed = 0;
-                bool fits = true;
-                for (int w = 0; w < 6; w++) {
-                    lnboff[6 * (size_t)m + w] = (int)lnbr.size();
-                    int cnt = 0;
-                    if (g.nbr_offsets) {
-                        for (int64_t q = g.nbr_offsets[6 * (size_t)l + w]; q < g.nbr_offsets[6 * (size_t)l + w + 1]; q++) {
-                            int c = g.node_cell[g.nbr_ids[q]];
-                            if (c < 0) continue;      // only leaves are ever matched
-                            lnbr.push_back(c); cnt++;
-                        }
-                    }
-                    if (cnt > 31) fits = false;
-                    else packed |= (unsigned)cnt << (5 * w);
-                }
-                if (!fits) packed = 0xFFFFFFFFu;
-                REQUIRE(lnbr.size() < (1ull << 31), "too many leaf neighbour entries");
-                float4 a, c;
-                a.x = (float)b[0]; a.y = (float)b[1]; a.z = (float)b[2]; std::memcpy(&a.w, &base, 4);
-                c.x = (float)b[3]; c.y = (float)b[4]; c.z = (float)b[5]; std::memcpy(&c.w, &packed, 4);
-                lr[2 * (size_t)m] = a; lr[2 * (size_t)m + 1] = c;
-            }
-            lnboff[6 * (size_t)nc] = (int)lnbr.size();
-            G.leafrec = upload(A, lr.data(), lr.size(), s);
-            G.lnbr = upload(A, lnbr.data(), lnbr.size(), s);
-            G.lnboff = upload(A, lnboff.data(), lnboff.size(), s);
+            RopeTree rt;
+            build_rope_tree(g, rt);
+            G.lrec = upload(A, rt.lrec.data(), rt.lrec.size(), s);
+            G.irec = upload(A, rt.irec.data(), std::max<size_t>(rt.irec.size(), 1), s);
+            G.cell_leaf = upload(A, rt.cell_leaf.data(), rt.cell_leaf.size(), s);
+            G.root_ref = rt.root_ref;
         }
         REQUIRE(g.search_method != SKG_SEARCH_BOOKKEEPING || g.type == SKG_GRID_OCTREE,
                 "the bookkeeping search method requires an octree");
@@ -292,6 +264,35 @@ double planck_B(double lambda, double T) {   // PlanckFunction.cpp:24-33
 
 }  // namespace
 
+// Device tables of one launch (header, work items, scene slots, wavelength list) and its
+// counters; filled from host memory before each launch.
+struct Staging {
+    BatchHeader* hdr = nullptr;
+    WorkItem* items = nullptr;
+    DevGrid* grids = nullptr;
+    const DevScene** scenes = nullptr;
+    int* ells = nullptr;
+    unsigned long long* work = nullptr;
+    unsigned* err = nullptr;
+    unsigned long long* counters = nullptr;
+    int max_items = 0, max_slots = 0, max_ells = 0;
+    void alloc(Allocs& A, int items, int slots, int nells) {
+        max_items = items; max_slots = slots; max_ells = nells;
+        hdr = A.alloc<BatchHeader>(1); this->items = A.alloc<WorkItem>(items); grids = A.alloc<DevGrid>(slots);
+        scenes = (const DevScene**)A.alloc<void*>(slots); ells = A.alloc<int>(nells);
+        work = A.alloc<unsigned long long>(1); err = A.alloc<unsigned>(1); counters = A.alloc<unsigned long long>(10);
+        if (!hdr || !this->items || !grids || !scenes || !ells || !work || !err || !counters)
+            throw Failure{SKG_ERR_OOM, "device allocation failed"};
+    }
+    RunParams params(int max_scatt) const {
+        RunParams P;
+        std::memset(&P, 0, sizeof(P));
+        P.hdr = hdr; P.items = items; P.grids = grids; P.scenes = scenes; P.ells = ells;
+        P.max_scatt = max_scatt; P.work = work; P.err = err; P.counters = counters;
+        return P;
+    }
+};
+
 struct skg_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -304,10 +305,9 @@ struct skg_ctx {
     int nlambda = 0, ncomp = 0;
     int64_t ncells = 0;
     std::vector<int64_t> cube_len, sed_len;
-    unsigned long long* counters = nullptr;
-    unsigned* err = nullptr;
-    unsigned long long* work = nullptr;
-    int* ells = nullptr; int ells_cap = 0;
+    unsigned long long* counters = nullptr;   // = own.counters
+    unsigned* err = nullptr;                  // = own.err
+    Staging own;                              // tables of this context's own launches
     std::vector<double> lambda, dlambda;
     // dust emission
     int nT = 0;
@@ -432,6 +432,7 @@ int skg_ctx_create(const skg_scene* sc, int device, skg_ctx** out) {
                 CK(cudaStreamSynchronize(s));
             }
             H.rhof = rf;
+            if (sc->ncomp == 1 && ctx->grid.lrec) CK(launch_embed_density(ctx->grid, rf, s));
         }
 
         // stellar system (StellarSystem.cpp:35-52)
@@ -551,9 +552,11 @@ int skg_ctx_create(const skg_scene* sc, int device, skg_ctx** out) {
             H.emit_Lv = ctx->emit_Lv; H.emit_cdf = ctx->emit_cdf; H.emit_Ltot = ctx->emit_Ltot;
         }
         ctx->sumbuf = zeros<double>(A, 2, s);
-        ctx->counters = zeros<unsigned long long>(A, 10, s);
-        ctx->err = zeros<unsigned>(A, 1, s);
-        ctx->work = zeros<unsigned long long>(A, 1, s);
+        ctx->own.alloc(A, 1, 1, nl);
+        CK(cudaMemsetAsync(ctx->own.counters, 0, 10 * sizeof(unsigned long long), s));
+        CK(cudaMemsetAsync(ctx->own.err, 0, sizeof(unsigned), s));
+        ctx->counters = ctx->own.counters;
+        ctx->err = ctx->own.err;
         ctx->ds = upload(A, &H, 1, s);
         CK(cudaStreamSynchronize(s));
         *out = ctx;
@@ -686,27 +689,29 @@ int skg_run_phase(skg_ctx* ctx, int phase, const int32_t* ells, int nell, uint64
         REQUIRE(count <= npp || npp == 0, "packet range exceeds the packet count");
         if (phase != SKG_PHASE_STELLAR) REQUIRE(ctx->emit_cdf != nullptr, "dust phases need dust emission enabled");
         cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-        if (nell > ctx->ells_cap) {
-            ctx->ells = ctx->A.alloc<int>(nell);
-            if (!ctx->ells) throw Failure{SKG_ERR_OOM, "device allocation failed"};
-            ctx->ells_cap = nell;
-        }
-        CK(cudaMemcpyAsync(ctx->ells, ells, nell * sizeof(int), cudaMemcpyHostToDevice, s));
-        CK(cudaMemsetAsync(ctx->work, 0, sizeof(unsigned long long), s));
-        CK(cudaMemsetAsync(ctx->err, 0, sizeof(unsigned), s));
-        RunParams P;
-        std::memset(&P, 0, sizeof(P));
-        P.phase = phase; P.ells = ctx->ells; P.nell = nell;
-        P.npp = count; P.first_packet = first_packet; P.Npp_total = npp; P.seed = seed;
-        P.max_scatt = (opts && opts->max_scatt > 0) ? opts->max_scatt : 100000;
-        P.work = ctx->work; P.err = ctx->err; P.counters = ctx->counters;
+        if (count == 0) return SKG_OK;
+        // one slot, one work item (pageable host sources: the copies are staged before return)
+        BatchHeader H = {phase, 1, 1, 0, (uint64_t)nell * count};
+        WorkItem W;
+        std::memset(&W, 0, sizeof(W));
+        W.slot = 0; W.nell = nell; W.ell0 = 0; W.npp_total = npp; W.first = first_packet; W.count = count;
+        W.seed = seed; W.begin = 0;
         DevGrid g = ctx->grid;
         if (opts && opts->max_steps > 0) g.max_steps = opts->max_steps;
+        const DevScene* sp = ctx->ds;
+        Staging& T = ctx->own;
+        CK(cudaMemcpyAsync(T.hdr, &H, sizeof(H), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(T.items, &W, sizeof(W), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(T.grids, &g, sizeof(g), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(T.scenes, &sp, sizeof(sp), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(T.ells, ells, nell * sizeof(int), cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(T.work, 0, sizeof(unsigned long long), s));
+        CK(cudaMemsetAsync(T.err, 0, sizeof(unsigned), s));
+        RunParams P = T.params((opts && opts->max_scatt > 0) ? opts->max_scatt : 100000);
         int precision = opts ? opts->precision : SKG_PREC_FP32;
         int blocks = opts ? opts->blocks : 0, threads = opts ? opts->threads : 0;
-        if (count == 0) return SKG_OK;
         CK(cudaEventRecord(ctx->ev0, s));
-        CK(launch_tracer(g, ctx->ds, P, precision, blocks, threads, s));
+        CK(launch_tracer(ctx->grid.type, P, 1, precision, blocks, threads, s));
         CK(cudaEventRecord(ctx->ev1, s));
         return SKG_OK;
     } catch (const Failure& f) { return fail(ctx, f); }
@@ -956,5 +961,222 @@ int skg_tree_grid(const skg_tree* T, skg_grid* grid) {
 }
 
 int skg_tree_destroy(skg_tree* T) { delete T; return SKG_OK; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// batched launches
+
+struct skg_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    Allocs A;
+    Staging T;
+    // pinned host mirrors of the tables (read by the copies of a replayed graph)
+    BatchHeader* h_hdr = nullptr;
+    WorkItem* h_items = nullptr;
+    DevGrid* h_grids = nullptr;
+    const DevScene** h_scenes = nullptr;
+    int* h_ells = nullptr;
+    cudaEvent_t copied = nullptr;          // the previous launch's tables have been read
+    cudaGraphExec_t graph = nullptr;
+    int g_type = -1, g_prec = -1, g_blocks = -1, g_threads = -1;
+    cudaStream_t g_stream = nullptr;
+    std::string error;
+};
+
+static int bfail(skg_batch* b, const Failure& f) {
+    set_error(f.msg);
+    if (b) b->error = f.msg;
+    return f.code;
+}
+
+extern "C" {
+
+int skg_batch_create(int device, int max_slots, int max_items, int max_ells, skg_batch** out) {
+    *out = nullptr;
+    skg_batch* b = new skg_batch();
+    try {
+        REQUIRE(max_slots >= 1 && max_slots <= MAX_SLOTS, "1..64 slots per batch");
+        REQUIRE(max_items >= 1 && max_ells >= 1, "batch table sizes must be positive");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); throw Failure{SKG_ERR_NO_DEVICE, "no CUDA device"}; }
+        REQUIRE(device >= 0 && device < ndev, "device index out of range");
+        b->device = device;
+        CK(cudaSetDevice(device));
+        CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&b->ev0)); CK(cudaEventCreate(&b->ev1));
+        CK(cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming));
+        b->T.alloc(b->A, max_items, max_slots, max_ells);
+        CK(cudaMemset(b->T.counters, 0, 10 * sizeof(unsigned long long)));
+        CK(cudaMemset(b->T.err, 0, sizeof(unsigned)));
+        CK(cudaMallocHost((void**)&b->h_hdr, sizeof(BatchHeader)));
+        CK(cudaMallocHost((void**)&b->h_items, max_items * sizeof(WorkItem)));
+        CK(cudaMallocHost((void**)&b->h_grids, max_slots * sizeof(DevGrid)));
+        CK(cudaMallocHost((void**)&b->h_scenes, max_slots * sizeof(void*)));
+        CK(cudaMallocHost((void**)&b->h_ells, max_ells * sizeof(int)));
+        CK(cudaEventRecord(b->copied, b->stream));
+        *out = b;
+        return SKG_OK;
+    } catch (const Failure& f) {
+        int rc = bfail(nullptr, f);
+        skg_batch_destroy(b);
+        return rc;
+    }
+}
+
+int skg_batch_destroy(skg_batch* b) {
+    if (!b) return SKG_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->g_stream) cudaStreamSynchronize(b->g_stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->g_stream) cudaStreamDestroy(b->g_stream);
+    b->A.release();
+    if (b->h_hdr) cudaFreeHost(b->h_hdr);
+    if (b->h_items) cudaFreeHost(b->h_items);
+    if (b->h_grids) cudaFreeHost(b->h_grids);
+    if (b->h_scenes) cudaFreeHost((void*)b->h_scenes);
+    if (b->h_ells) cudaFreeHost(b->h_ells);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->copied) cudaEventDestroy(b->copied);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return SKG_OK;
+}
+
+int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, const skg_run_opts* opts, int flags,
+                  void* stream) {
+    if (!b) return SKG_ERR_INVALID;
+    try {
+        CK(cudaSetDevice(b->device));
+        REQUIRE(phase >= SKG_PHASE_STELLAR && phase <= SKG_PHASE_DUST_EMISSION, "unknown phase");
+        REQUIRE(nwork >= 0 && nwork <= b->T.max_items, "too many work items for this batch");
+        cudaStream_t s = stream ? (cudaStream_t)stream : b->stream;
+        // the pinned tables may still be read by the previous launch's copies
+        CK(cudaEventSynchronize(b->copied));
+        int nslots = 0, nells = 0, gtype = -1;
+        uint64_t total = 0;
+        std::vector<skg_ctx*> slots;
+        for (int i = 0; i < nwork; i++) {
+            const skg_work& w = work[i];
+            REQUIRE(w.ctx != nullptr && w.ells && w.nell > 0, "work item needs a context and wavelengths");
+            REQUIRE(w.ctx->device == b->device, "all contexts must live on the batch's device");
+            REQUIRE(w.count <= w.npp, "packet range exceeds the packet count");
+            if (gtype < 0) gtype = w.ctx->grid.type;
+            auto tree = [](int t) { return t == SKG_GRID_OCTREE || t == SKG_GRID_BINTREE; };
+            REQUIRE(w.ctx->grid.type == gtype || (tree(gtype) && tree(w.ctx->grid.type)),
+                    "a batch holds one kind of grid");
+            if (phase != SKG_PHASE_STELLAR) REQUIRE(w.ctx->emit_cdf != nullptr, "dust phases need dust emission enabled");
+            int slot = -1;
+            for (int q = 0; q < nslots; q++) if (slots[q] == w.ctx) slot = q;
+            if (slot < 0) {
+                REQUIRE(nslots < b->T.max_slots, "too many distinct simulations for this batch");
+                slot = nslots++;
+                slots.push_back(w.ctx);
+                DevGrid g = w.ctx->grid;
+                if (opts && opts->max_steps > 0) g.max_steps = opts->max_steps;
+                b->h_grids[slot] = g;
+                b->h_scenes[slot] = w.ctx->ds;
+            }
+            REQUIRE(nells + w.nell <= b->T.max_ells, "too many wavelength entries for this batch");
+            WorkItem& W = b->h_items[i];
+            std::memset(&W, 0, sizeof(W));
+            W.slot = slot; W.nell = w.nell; W.ell0 = nells; W.npp_total = w.npp; W.first = w.first; W.count = w.count;
+            W.seed = w.seed; W.begin = total;
+            for (int e = 0; e < w.nell; e++) {
+                REQUIRE(w.ells[e] >= 0 && w.ells[e] < w.ctx->nlambda, "wavelength index out of range");
+                b->h_ells[nells + e] = w.ells[e];
+            }
+            nells += w.nell;
+            total += (uint64_t)w.nell * w.count;
+        }
+        *b->h_hdr = BatchHeader{phase, nslots, nwork, 0, total};
+        int precision = opts ? opts->precision : SKG_PREC_FP32;
+        int blocks = opts ? opts->blocks : 0, threads = opts ? opts->threads : 0;
+        if (blocks <= 0) {
+            int sms = 0;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+            blocks = sms * 3;       // three 256-thread blocks per SM (the tracer's launch bounds)
+        }
+        if (threads <= 0) threads = 256;
+        RunParams P = b->T.params((opts && opts->max_scatt > 0) ? opts->max_scatt : 100000);
+        Staging& T = b->T;
+        auto enqueue = [&](cudaStream_t q) {
+            CK(cudaMemcpyAsync(T.hdr, b->h_hdr, sizeof(BatchHeader), cudaMemcpyHostToDevice, q));
+            CK(cudaMemcpyAsync(T.items, b->h_items, T.max_items * sizeof(WorkItem), cudaMemcpyHostToDevice, q));
+            CK(cudaMemcpyAsync(T.grids, b->h_grids, T.max_slots * sizeof(DevGrid), cudaMemcpyHostToDevice, q));
+            CK(cudaMemcpyAsync(T.scenes, b->h_scenes, T.max_slots * sizeof(void*), cudaMemcpyHostToDevice, q));
+            CK(cudaMemcpyAsync(T.ells, b->h_ells, T.max_ells * sizeof(int), cudaMemcpyHostToDevice, q));
+            CK(cudaMemsetAsync(T.work, 0, sizeof(unsigned long long), q));
+            CK(cudaMemsetAsync(T.err, 0, sizeof(unsigned), q));
+            // every slot's DevGrid is copied into shared memory: size for the batch's capacity
+            CK(launch_tracer(gtype < 0 ? SKG_GRID_CARTESIAN : gtype, P, T.max_slots, precision, blocks, threads, q));
+        };
+        CK(cudaEventRecord(b->ev0, s));
+        if (flags & SKG_BATCH_GRAPH) {
+            bool same = b->graph && b->g_type == gtype && b->g_prec == precision && b->g_blocks == blocks &&
+                        b->g_threads == threads;
+            if (!same) {
+                if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+                if (!b->g_stream) CK(cudaStreamCreateWithFlags(&b->g_stream, cudaStreamNonBlocking));
+                cudaGraph_t gr;
+                CK(cudaStreamBeginCapture(b->g_stream, cudaStreamCaptureModeThreadLocal));
+                enqueue(b->g_stream);
+                CK(cudaStreamEndCapture(b->g_stream, &gr));
+                cudaError_t e = cudaGraphInstantiate(&b->graph, gr, 0);
+                cudaGraphDestroy(gr);
+                CK(e);
+                b->g_type = gtype; b->g_prec = precision; b->g_blocks = blocks; b->g_threads = threads;
+            }
+            CK(cudaGraphLaunch(b->graph, s));
+        } else {
+            enqueue(s);
+        }
+        CK(cudaEventRecord(b->ev1, s));
+        CK(cudaEventRecord(b->copied, s));
+        return SKG_OK;
+    } catch (const Failure& f) { return bfail(b, f); }
+}
+
+int skg_batch_sync(skg_batch* b, int timeout_ms) {
+    if (!b) return SKG_ERR_INVALID;
+    cudaSetDevice(b->device);
+    auto t0 = std::chrono::steady_clock::now();
+    while (true) {
+        cudaError_t e = cudaEventQuery(b->ev1);
+        if (e == cudaSuccess) break;
+        if (e != cudaErrorNotReady) { cudaGetLastError(); return bfail(b, Failure{SKG_ERR_CUDA, cudaGetErrorString(e)}); }
+        if (timeout_ms >= 0 && std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() > timeout_ms)
+            return bfail(b, Failure{SKG_ERR_TIMEOUT, "timed out waiting for the device"});
+        std::this_thread::sleep_for(std::chrono::microseconds(100));
+    }
+    unsigned err = 0;
+    cudaMemcpy(&err, b->T.err, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    if (err & ERR_NAN_TAU) return bfail(b, Failure{SKG_ERR_NAN_TAU, "The optical depth along the path is not a positive number"});
+    if (err & (ERR_STEP_BUDGET | ERR_SCATT_BUDGET)) return bfail(b, Failure{SKG_ERR_STEP_BUDGET, "a packet exceeded its step or scattering budget"});
+    return SKG_OK;
+}
+
+int skg_batch_counters(skg_batch* b, skg_counters* out) {
+    if (!b || !out) return SKG_ERR_INVALID;
+    int rc = skg_batch_sync(b, -1);
+    unsigned long long c[10];
+    cudaMemcpy(c, b->T.counters, sizeof(c), cudaMemcpyDeviceToHost);
+    out->packets = c[0]; out->steps = c[1]; out->traversals = c[2]; out->scatterings = c[3]; out->peeloffs = c[4];
+    out->absorb_adds = c[5]; out->pixel_adds = c[6]; out->nbr_scanned = c[7]; out->fallbacks = c[8]; out->errors = c[9];
+    return rc;
+}
+
+int skg_batch_last_ms(skg_batch* b, float* ms) {
+    if (!b || !ms) return SKG_ERR_INVALID;
+    cudaSetDevice(b->device);
+    cudaError_t e = cudaEventSynchronize(b->ev1);
+    if (e != cudaSuccess) { cudaGetLastError(); return bfail(b, Failure{SKG_ERR_CUDA, cudaGetErrorString(e)}); }
+    cudaEventElapsedTime(ms, b->ev0, b->ev1);
+    return SKG_OK;
+}
 
 }  // extern "C"

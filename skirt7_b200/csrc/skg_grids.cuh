@@ -42,14 +42,13 @@ struct DevGrid {
     const int*    nbr;
     const int*    cell_node;    // leaf node of each cell (TreeDustGrid::_idv)
     int search;
-    // FP32 walk: one 32-byte record per leaf, indexed by cell number,
-    //   leafrec[2m]   = (xmin, ymin, zmin, int offset of the leaf's neighbour block in lnbr)
-    //   leafrec[2m+1] = (xmax, ymax, zmax, uint per-wall neighbour counts, 5 bits each, or ~0u)
-    // lnbr holds neighbour CELL numbers grouped by wall; lnboff[6m+w] are the per-wall offsets
-    // (read only when a wall has more than 31 neighbours).
-    const float4* leafrec;
-    const int*    lnbr;
-    const int*    lnboff;
+    // FP32 walk on the rope-linked tree (build_rope_tree): 64-byte leaf records in depth-first
+    // order holding box, density, cell number and one rope per wall; 48-byte internal records
+    // holding the split point and the child references
+    const float4* lrec;
+    const float4* irec;
+    const int*    cell_leaf;    // cell number -> leaf index
+    int root_ref;
 
     // Voronoi: sites (3 doubles / float4), CSR neighbours, FP32 bisector planes per CSR entry
     // vplane[q] = (n.x, n.y, n.z, n.p) with n = p_i - p_r and p the bisector midpoint; walls are
@@ -146,6 +145,7 @@ struct CartStepper {
     int steps;
     int cell0;                  // cell holding the start position (-1 if it lies outside the grid)
     static constexpr int scanned = 0, fallbacks = 0;
+    static constexpr float rho = -1.f;   // density not embedded: the tracer reads it by cell
 
     // hint: a cell known to hold the start position (or -1); it is verified against the planes
     SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz, int hint = -1) {
@@ -286,6 +286,7 @@ struct TreeNodeWalk {
     int fallbacks;
     int scanned;
     int cell0;
+    static constexpr float rho = -1.f;
 
     SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz, int hint = -1) {
         kx = dx; ky = dy; kz = dz; npend = 0; ipend = 0; done = false; steps = 0; fallbacks = 0; scanned = 0;
@@ -432,41 +433,62 @@ template<typename R> struct TreeStepper : TreeNodeWalk<R> {};
 template<>
 struct TreeStepper<float> {
     float x, y, z, kx, ky, kz;
-    int cell;
-    float4 lo, hi;
-    int node;                   // node-based walk (search methods other than Neighbor)
+    float4 r0, r1, r2, r3;      // the current leaf's record
+    int leaf;
     float pend[3]; int npend, ipend;
     bool done;
     int steps, fallbacks, scanned;
     int cell0;
+    float rho;                  // density embedded in the record of the last segment's cell
     TreeNodeWalk<float> bk;     // Bookkeeping search (octree index arithmetic)
 
-    SKG_D void load(const DevGrid& g, int m) { lo = __ldg(g.leafrec + 2 * (size_t)m); hi = __ldg(g.leafrec + 2 * (size_t)m + 1); }
-    SKG_D static bool inbox(float4 a, float4 b, float px, float py, float pz) {
-        return px >= a.x && px <= b.x && py >= a.y && py <= b.y && pz >= a.z && pz <= b.z;
+    SKG_D void load(const DevGrid& g, int li) {
+        const float4* p = g.lrec + 4 * (size_t)li;
+        r0 = __ldg(p); r1 = __ldg(p + 1); r2 = __ldg(p + 2); r3 = __ldg(p + 3);
     }
-    SKG_D int descend(const DevGrid& g, float px, float py, float pz) {
-        int l = tree_whichnode<float>(g, px, py, pz);
-        return l >= 0 ? g.node_cell[l] : -1;
+    SKG_D bool inside(float px, float py, float pz) const {
+        return px >= r0.x && px <= r1.x && py >= r0.y && py <= r1.y && pz >= r0.z && pz <= r1.z;
+    }
+    // descends from a node reference to the leaf holding the point (the reference's child(r)
+    // rule: a point on a split plane belongs to the upper child)
+    SKG_D static int descend(const DevGrid& g, int ref, float px, float py, float pz) {
+        int guard = 0;
+        while (ref < -1 && guard++ < 64) {
+            const float4* p = g.irec + 3 * (size_t)(-ref - 2);
+            float4 a = __ldg(p);
+            int d = __float_as_int(a.w), c;
+            if (d < 0) c = (px < a.x ? 0 : 1) + (py < a.y ? 0 : 2) + (pz < a.z ? 0 : 4);
+            else c = ((d == 0 ? px < a.x : d == 1 ? py < a.y : pz < a.z) ? 0 : 1);
+            float4 b = __ldg(p + 1 + (c >> 2));
+            int k = c & 3;
+            ref = __float_as_int(k == 0 ? b.x : k == 1 ? b.y : k == 2 ? b.z : b.w);
+        }
+        return ref;
+    }
+    SKG_D static int locate(const DevGrid& g, float px, float py, float pz) {
+        if (!(px >= (float)g.xmin && px <= (float)g.xmax && py >= (float)g.ymin && py <= (float)g.ymax &&
+              pz >= (float)g.zmin && pz <= (float)g.zmax)) return -1;
+        return descend(g, g.root_ref, px, py, pz);
     }
 
     SKG_D void init(const DevGrid& g, float rx, float ry, float rz, float dx, float dy, float dz, int hint = -1) {
         kx = dx; ky = dy; kz = dz; npend = 0; ipend = 0; done = false; steps = 0; fallbacks = 0; scanned = 0;
-        cell0 = -1;
+        cell0 = -1; rho = -1.f;
         if (g.search == SKG_SEARCH_BOOKKEEPING) {
             bk.init(g, rx, ry, rz, dx, dy, dz, hint);
             cell0 = bk.cell0; done = bk.done;
             return;
         }
         if (hint >= 0) {
-            load(g, hint);
-            if (inbox(lo, hi, rx, ry, rz)) { cell = hint; cell0 = hint; x = rx; y = ry; z = rz; return; }
+            leaf = __ldg(g.cell_leaf + hint);
+            load(g, leaf);
+            if (inside(rx, ry, rz)) { cell0 = hint; x = rx; y = ry; z = rz; return; }
         }
         bool ok = move_inside<float>(g, g.epsf, rx, ry, rz, kx, ky, kz, pend, npend);
-        cell = ok ? descend(g, rx, ry, rz) : -1;
-        if (cell < 0) { npend = 0; done = true; return; }
-        if (npend == 0) cell0 = cell;
-        load(g, cell);
+        leaf = ok ? locate(g, rx, ry, rz) : -1;
+        if (leaf < 0) { npend = 0; done = true; return; }
+        load(g, leaf);
+        if (npend == 0) cell0 = __float_as_int(r1.w);
         x = rx; y = ry; z = rz;
     }
 
@@ -476,56 +498,47 @@ struct TreeStepper<float> {
             steps = bk.steps; done = bk.done;
             return r;
         }
-        if (ipend < npend) { m = -1; ds = pend[ipend++]; return true; }
+        if (ipend < npend) { m = -1; ds = pend[ipend++]; rho = 0.f; return true; }
         const float eps = g.epsf;
         while (!done) {
             if (++steps > g.max_steps) { done = true; return false; }
-            float xnext = (kx < 0.f) ? lo.x : hi.x;
-            float ynext = (ky < 0.f) ? lo.y : hi.y;
-            float znext = (kz < 0.f) ? lo.z : hi.z;
+            float xnext = (kx < 0.f) ? r0.x : r1.x;
+            float ynext = (ky < 0.f) ? r0.y : r1.y;
+            float znext = (kz < 0.f) ? r0.z : r1.z;
             float dsx = (fabsf(kx) > 1e-15f) ? (xnext - x) / kx : FLT_MAX;
             float dsy = (fabsf(ky) > 1e-15f) ? (ynext - y) / ky : FLT_MAX;
             float dsz = (fabsf(kz) > 1e-15f) ? (znext - z) / kz : FLT_MAX;
-            float d; int wall;
-            if (dsx <= dsy && dsx <= dsz) { d = dsx; wall = (kx < 0.f) ? 0 : 1; }
-            else if (dsy <= dsx && dsy <= dsz) { d = dsy; wall = (ky < 0.f) ? 2 : 3; }
-            else { d = dsz; wall = (kz < 0.f) ? 4 : 5; }
-            m = cell;
+            float d; int rope;
+            if (dsx <= dsy && dsx <= dsz) { d = dsx; rope = __float_as_int((kx < 0.f) ? r2.x : r2.y); }
+            else if (dsy <= dsx && dsy <= dsz) { d = dsy; rope = __float_as_int((ky < 0.f) ? r2.z : r2.w); }
+            else { d = dsz; rope = __float_as_int((kz < 0.f) ? r3.x : r3.y); }
+            m = __float_as_int(r1.w);
+            rho = r0.w;
             x += (d + eps) * kx; y += (d + eps) * ky; z += (d + eps) * kz;
-            // neighbours across the exit wall (TreeNode::whichnode(wall, r), TreeNode.cpp:84-93)
-            unsigned packed = __float_as_uint(hi.w);
-            int base = __float_as_int(lo.w), q0, cnt;
-            if (packed != 0xFFFFFFFFu) {
-                int pre = 0;
-                for (int w = 0; w < wall; w++) pre += (packed >> (5 * w)) & 31u;
-                q0 = base + pre; cnt = (packed >> (5 * wall)) & 31u;
-            } else {
-                q0 = g.lnboff[6 * cell + wall]; cnt = g.lnboff[6 * cell + wall + 1] - q0;
+            // follow the rope of the exit wall; if the point is not in the leaf it leads to (it
+            // crossed near an edge or corner), locate it from the root
+            int next = (rope == -1) ? -1 : descend(g, rope, x, y, z);
+            scanned++;
+            if (next >= 0) {
+                load(g, next);
+                if (!inside(x, y, z)) {
+                    next = locate(g, x, y, z); fallbacks++;
+                    if (next >= 0) load(g, next);
+                }
+            } else if (rope != -1) {
+                next = locate(g, x, y, z); fallbacks++;
+                if (next >= 0) load(g, next);
             }
-            int found = -1;
-            float4 nlo, nhi;
-            if (g.search == SKG_SEARCH_TOPDOWN) cnt = 0;   // TopDown: always from the root
-            for (int q = 0; q < cnt; q++) {
-                int c = __ldg(g.lnbr + q0 + q);
-                scanned++;
-                nlo = __ldg(g.leafrec + 2 * (size_t)c); nhi = __ldg(g.leafrec + 2 * (size_t)c + 1);
-                if (inbox(nlo, nhi, x, y, z)) { found = c; break; }
-            }
-            if (found < 0) {                       // rounding near a corner: search from the root
-                found = descend(g, x, y, z);
-                if (g.search != SKG_SEARCH_TOPDOWN) fallbacks++;
-                if (found >= 0) { nlo = __ldg(g.leafrec + 2 * (size_t)found); nhi = __ldg(g.leafrec + 2 * (size_t)found + 1); }
-            }
-            if (found == cell) {                   // stuck (TreeDustGrid.cpp:476-493)
+            if (next == leaf) {                    // stuck (TreeDustGrid.cpp:476-493)
                 x = nextafterf(x, (kx < 0.f) ? -FLT_MAX : FLT_MAX);
                 y = nextafterf(y, (ky < 0.f) ? -FLT_MAX : FLT_MAX);
                 z = nextafterf(z, (kz < 0.f) ? -FLT_MAX : FLT_MAX);
-                found = descend(g, x, y, z);
-                if (found == cell) found = -1;
-                else if (found >= 0) { nlo = __ldg(g.leafrec + 2 * (size_t)found); nhi = __ldg(g.leafrec + 2 * (size_t)found + 1); }
+                next = locate(g, x, y, z);
+                if (next == leaf) next = -1;
+                else if (next >= 0) load(g, next);
             }
-            if (found < 0) done = true;
-            else { cell = found; lo = nlo; hi = nhi; d += eps; }   // the nudge is credited to this segment
+            if (next < 0) done = true;
+            else { leaf = next; d += eps; }      // the nudge is credited to the segment left behind
             if (d > 0.f) { ds = d; return true; }
         }
         return false;
@@ -577,6 +590,7 @@ struct VoronoiStepper {
     int fallbacks;
     int scanned;
     int cell0;
+    static constexpr float rho = -1.f;
 
     // hint: the cell holding the start position (the interaction point lies in the cell of its
     // segment); accepted for a position strictly inside the domain

@@ -302,6 +302,94 @@ void Tree::build(int min_level, int max_level, double max_mass_fraction, double 
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Rope-linked tree for the FP32 walk.
+//
+// Leaves are numbered in depth-first order (children in order: for an octree the Morton order of
+// the leaves), so that leaves met in sequence along a ray sit close together in memory.  Each
+// leaf face carries a rope: the deepest node beyond the face whose box covers the whole face
+// (Havran's neighbour links).  A step then follows the rope of the exit wall -- to the next leaf
+// directly, or to a node from which the point descends one or two levels.
+void build_rope_tree(const skg_grid& g, RopeTree& out) {
+    const int n = g.nnodes;
+    std::vector<int> ref(n, -1);
+    std::vector<int> order;            // depth-first visit order
+    order.reserve(n);
+    std::vector<int> stack{0};
+    int nleaf = 0, nint = 0;
+    while (!stack.empty()) {
+        int l = stack.back(); stack.pop_back();
+        order.push_back(l);
+        int c0 = g.node_child[l];
+        if (c0 < 0) { ref[l] = nleaf++; continue; }
+        ref[l] = -(nint++ + 2);
+        int nch = (g.node_dir[l] < 0) ? 8 : 2;
+        for (int c = nch - 1; c >= 0; c--) stack.push_back(c0 + c);
+    }
+    out.root_ref = ref[0];
+    out.lrec.assign(4 * (size_t)nleaf, float4{0, 0, 0, 0});
+    out.irec.assign(3 * (size_t)nint, float4{0, 0, 0, 0});
+    int ncells = 0;
+    for (int l = 0; l < n; l++) if (g.node_cell[l] >= 0) ncells = std::max(ncells, g.node_cell[l] + 1);
+    out.cell_leaf.assign(ncells, -1);
+    const double ext[6] = {g.xmin, g.ymin, g.zmin, g.xmax, g.ymax, g.zmax};
+    auto box = [&](int l) { return g.node_box + 6 * (size_t)l; };
+    auto as_f = [](int v) { float f; std::memcpy(&f, &v, 4); return f; };
+
+    for (int l : order) {
+        const double* b = box(l);
+        int c0 = g.node_child[l];
+        if (c0 >= 0) {
+            int j = -ref[l] - 2;
+            const double* s = box(c0);           // the split point is child 0's upper corner
+            int d = g.node_dir[l];
+            int nch = (d < 0) ? 8 : 2;
+            int ch[8];
+            for (int c = 0; c < 8; c++) ch[c] = (c < nch) ? ref[c0 + c] : -1;
+            out.irec[3 * (size_t)j] = float4{(float)s[3], (float)s[4], (float)s[5], as_f(d)};
+            out.irec[3 * (size_t)j + 1] = float4{as_f(ch[0]), as_f(ch[1]), as_f(ch[2]), as_f(ch[3])};
+            out.irec[3 * (size_t)j + 2] = float4{as_f(ch[4]), as_f(ch[5]), as_f(ch[6]), as_f(ch[7])};
+            continue;
+        }
+        int li = ref[l];
+        int rope[6];
+        for (int w = 0; w < 6; w++) {
+            int a = w / 2;
+            bool up = (w % 2) == 1;
+            double c = up ? b[a + 3] : b[a];
+            if ((up && c >= ext[a + 3]) || (!up && c <= ext[a])) { rope[w] = -1; continue; }
+            // descend from the root while one child covers the whole face region
+            int node = 0;
+            while (g.node_child[node] >= 0) {
+                int k0 = g.node_child[node];
+                const double* sp = box(k0);
+                int d = g.node_dir[node];
+                int sel = 0;
+                bool split_face = false;
+                for (int ax = 0; ax < 3 && !split_face; ax++) {
+                    if (d >= 0 && ax != d) continue;
+                    double s = sp[ax + 3];
+                    bool upper;
+                    if (ax == a) upper = up ? (c >= s) : (c > s);   // the slab just beyond the face
+                    else if (b[ax + 3] <= s) upper = false;
+                    else if (b[ax] >= s) upper = true;
+                    else { split_face = true; break; }
+                    if (upper) sel |= (d < 0) ? (1 << ax) : 1;
+                }
+                if (split_face) break;
+                node = k0 + sel;
+            }
+            rope[w] = ref[node];
+        }
+        int cell = g.node_cell[l];
+        out.cell_leaf[cell] = li;
+        out.lrec[4 * (size_t)li] = float4{(float)b[0], (float)b[1], (float)b[2], 0.f};
+        out.lrec[4 * (size_t)li + 1] = float4{(float)b[3], (float)b[4], (float)b[5], as_f(cell)};
+        out.lrec[4 * (size_t)li + 2] = float4{as_f(rope[0]), as_f(rope[1]), as_f(rope[2]), as_f(rope[3])};
+        out.lrec[4 * (size_t)li + 3] = float4{as_f(rope[4]), as_f(rope[5]), 0.f, 0.f};
+    }
+}
+
 // Builds the topology from explicit decisions (split[l] for node l in creation order).
 void Tree::build_from_splits(const uint8_t* splitv, int64_t nsplit) {
     nodes.clear();

@@ -13,8 +13,8 @@ struct DevScene;
 struct RunParams;
 
 // skg_tracer.cu
-cudaError_t launch_tracer(const DevGrid& g, const DevScene* dS, const RunParams& P, int precision,
-                          int blocks, int threads, cudaStream_t stream);
+cudaError_t launch_tracer(int grid_type, const RunParams& P, int nslots, int precision, int blocks, int threads,
+                          cudaStream_t stream);
 
 // skg_trace.cu (compiled with --fmad=false: bit-exact FP64 traversal)
 cudaError_t launch_count_segments(const DevGrid& g, const double* r, const double* k, int64_t n,
@@ -42,6 +42,7 @@ cudaError_t launch_emission_sources(const DevScene* dS, int nlambda, int ncells,
                                     cudaStream_t s);
 size_t emission_scan_scratch_bytes(int ncells);
 cudaError_t launch_sum(const double* x, int64_t n, double* out, cudaStream_t s);
+cudaError_t launch_embed_density(const DevGrid& g, const float* rhof, cudaStream_t s);
 cudaError_t launch_voronoi_cells(const double* sites, int nsites, const double* ext, const int* gcell_off,
                                  const int* gcell_ids, int gn, int kmax, int* nbr_count, int* nbr_ids,
                                  double* volume, double* centroid, double* bbox, int* status,

@@ -78,15 +78,36 @@ struct DevScene {
     double dust_emission_bias;
 };
 
-// Per-launch parameters.
-struct RunParams {
-    int phase;
-    const int* ells;          // device array of wavelength indices
+// One launch carries slices of one or more simulations ("slots").  A work item is one slice: the
+// packets [first, first+count) of every listed wavelength of the simulation in `slot`, each with
+// luminosity L/npp_total.  Global packet index p belongs to the item with begin <= p < begin +
+// count*nell.  The header and the tables live in device memory so that a captured launch can be
+// replayed with new contents.
+struct WorkItem {
+    int slot;
     int nell;
-    uint64_t npp;             // packets per wavelength in this launch
-    uint64_t first_packet;    // packet id offset (sharding)
-    uint64_t Npp_total;       // the definitive packet count per wavelength (L per packet = L/Npp_total)
+    int ell0;                 // wavelengths: ells[ell0 .. ell0 + nell)
+    int pad;
+    uint64_t npp_total;
+    uint64_t first, count;
     uint64_t seed;
+    uint64_t begin;
+};
+struct BatchHeader {
+    int phase;
+    int nslots;
+    int nitems;
+    int pad;
+    uint64_t total;           // packets of all items
+};
+constexpr int MAX_SLOTS = 64;
+
+struct RunParams {
+    const BatchHeader* hdr;
+    const WorkItem* items;
+    const DevGrid* grids;         // [nslots]
+    const DevScene* const* scenes; // [nslots]
+    const int* ells;
     int max_scatt;
     unsigned long long* work;     // packet work counter
     unsigned int* err;            // error word

@@ -190,6 +190,21 @@ cudaError_t launch_emission_sources(const DevScene*, int nl, int nc, const doubl
     return cudaGetLastError();
 }
 
+// Writes each leaf's (single-component) density into its rope-tree record, so that a cell step
+// of the FP32 walk reads box, density and ropes in one 64-byte gather.
+__global__ void embed_density_kernel(float4* lrec, int nleaves, const float* __restrict__ rhof) {
+    int li = blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= nleaves) return;
+    int cell = __float_as_int(lrec[4 * (size_t)li + 1].w);
+    lrec[4 * (size_t)li].w = rhof[cell];
+}
+cudaError_t launch_embed_density(const DevGrid& g, const float* rhof, cudaStream_t s) {
+    int n = g.ncells;
+    if (n <= 0) return cudaSuccess;
+    embed_density_kernel<<<(n + 255) / 256, 256, 0, s>>>(const_cast<float4*>(g.lrec), n, rhof);
+    return cudaGetLastError();
+}
+
 // Sum of a vector (absorbed-luminosity totals for the self-absorption convergence test).
 __global__ void sum_kernel(const double* __restrict__ x, int64_t n, double* out) {
     __shared__ double sh[256];

@@ -1,9 +1,10 @@
 // skg_tracer.cu -- the persistent photon-packet tracer.
 //
 // One launch runs a whole phase (stellar emission, dust self-absorption or dust emission) for a
-// batch of wavelengths: it replaces Parallel::call(this, &dostellaremissionchunk, Nlambda, Nchunks)
-// (MonteCarloSimulation.cpp:241-295) and the two dust chunk bodies (PanMonteCarloSimulation.cpp:
-// 191-346).  Each thread carries one packet at a time through an explicit state machine:
+// batch of wavelengths of one or more simulations: it replaces
+// Parallel::call(this, &dostellaremissionchunk, Nlambda, Nchunks) (MonteCarloSimulation.cpp:241-295)
+// and the two dust chunk bodies (PanMonteCarloSimulation.cpp:191-346).  Each thread carries one
+// packet at a time through an explicit state machine:
 //
 //   FETCH -> launch -> PEEL(emission) x groups -> MAIN1 -> [terminate?] -> MAIN2 -> PEEL(scattering)
 //         -> SCATTER -> MAIN1 -> ...
@@ -17,14 +18,16 @@
 //         interpolates inside that segment -- DustGridPath::pathlength (DustGridPath.cpp:162-173);
 //   PEEL  accumulates the optical depth towards an observer (DustSystem::opticaldepth, :960-976).
 // Instruments seen from the same direction share one peel-off traversal (identical optical
-// depth; the reference recomputes it per instrument).
+// depth; the reference recomputes it per instrument).  The event code (launch samplers,
+// scattering, detection) sits in non-inlined functions so that the step loop keeps few registers.
 #include "skg_scene.cuh"
 #include "skg_internal.h"
 
 namespace skg {
 
-enum Mode : int { M_FETCH = 0, M_PEEL_NEXT, M_MAIN1_START, M_AFTER_MAIN1, M_AFTER_MAIN2, M_SCATTER, M_DONE };
+enum Mode : int { M_FETCH = 0, M_LAUNCH, M_PEEL_NEXT, M_MAIN1_START, M_AFTER_MAIN1, M_AFTER_MAIN2, M_SCATTER, M_DONE };
 enum Trav : int { T_NONE = 0, T_PEEL, T_MAIN1, T_MAIN2 };
+enum Cnt : int { C_PACKETS = 0, C_STEPS, C_TRAV, C_SCATT, C_PEEL, C_ABS, C_PIX, C_NBR, C_FB, C_ERR, C_N };
 
 template<typename R> SKG_D double rho_load(const DevScene& S, size_t i);
 template<> SKG_D double rho_load<double>(const DevScene& S, size_t i) { return __ldg(S.rho + i); }
@@ -39,27 +42,29 @@ template<typename R> SKG_D double kappa_rho(const DevScene& S, int m, int ell) {
     return r;
 }
 
-// Instrument::detect for the members of one direction group after the shared traversal.
-SKG_D void detect_group(const DevScene& S, int grp, int ell, double Lpeel, double tau, int nscatt_peel,
-                        bool stellar, double x, double y, double z, unsigned& c_pix) {
-    double extf = exp(-tau);
-    double Lextf = Lpeel * extf;
+// Instrument::detect for the members of one direction group after the shared traversal
+// (SEDInstrument.cpp:32-42, FrameInstrument.cpp:33-47, SimpleInstrument.cpp:35-49,
+// FullInstrument.cpp:109-177).  Returns the number of tally updates.
+__device__ __noinline__ int detect_group(const DevScene& S, int grp, int ell, double Lpeel, double tau,
+                                         int nscatt_peel, bool stellar, double x, double y, double z) {
+    double Lextf = Lpeel * exp(-tau);
     const int nl = S.nlambda;
+    int adds = 0;
     for (int q = S.group_start[grp]; q < S.group_start[grp + 1]; q++) {
         const DevInstr& I = S.instr[S.group_instr[q]];
         int l = (I.type == SKG_INSTR_SED) ? -1 : pixel_on_detector(I, x, y, z);
         size_t fp = (size_t)I.nxp * I.nyp;
-        if (I.type == SKG_INSTR_FRAME) {                       // FrameInstrument.cpp:33-47
-            if (l >= 0) { atomicAdd(I.cube + (size_t)ell * fp + l, Lextf); c_pix++; }
-        } else if (I.type == SKG_INSTR_SED) {                  // SEDInstrument.cpp:32-42
-            atomicAdd(I.sed + ell, Lextf); c_pix++;
-        } else if (I.type == SKG_INSTR_SIMPLE) {               // SimpleInstrument.cpp:35-49
-            atomicAdd(I.sed + ell, Lextf); c_pix++;
-            if (l >= 0) { atomicAdd(I.cube + (size_t)ell * fp + l, Lextf); c_pix++; }
-        } else {                                               // FullInstrument.cpp:109-177
+        if (I.type == SKG_INSTR_FRAME) {
+            if (l >= 0) { atomicAdd(I.cube + (size_t)ell * fp + l, Lextf); adds++; }
+        } else if (I.type == SKG_INSTR_SED) {
+            atomicAdd(I.sed + ell, Lextf); adds++;
+        } else if (I.type == SKG_INSTR_SIMPLE) {
+            atomicAdd(I.sed + ell, Lextf); adds++;
+            if (l >= 0) { atomicAdd(I.cube + (size_t)ell * fp + l, Lextf); adds++; }
+        } else {
             auto add = [&](int c, double v) {
-                atomicAdd(I.sed + (size_t)c * nl + ell, v); c_pix++;
-                if (l >= 0) { atomicAdd(I.cube + ((size_t)c * nl + ell) * fp + l, v); c_pix++; }
+                atomicAdd(I.sed + (size_t)c * nl + ell, v); adds++;
+                if (l >= 0) { atomicAdd(I.cube + ((size_t)c * nl + ell) * fp + l, v); adds++; }
             };
             add(SKG_FULL_TOT, Lextf);
             if (stellar) {
@@ -73,6 +78,7 @@ SKG_D void detect_group(const DevScene& S, int grp, int ell, double Lpeel, doubl
             }
         }
     }
+    return adds;
 }
 
 // Does the group need a traversal?  Frame-only groups skip it when the packet projects off every
@@ -84,23 +90,150 @@ SKG_D bool group_needs_traversal(const DevScene& S, int grp, double x, double y,
     return false;
 }
 
+struct Launched { double x, y, z, kx, ky, kz, L, Lth; int ok; int stellar; };
+
+// Packet launch: StellarSystem::launch (StellarSystem.cpp:116-158) with the geometry samplers
+// (GeometricStellarComp.cpp:75-81), or a dust-emission launch from the cell luminosity CDF
+// (PanMonteCarloSimulation.cpp:216-224 self-absorption, :301-323 emission with bias).
+__device__ __noinline__ Launched launch_packet(const DevGrid& g, const DevScene& S, int phase, int ell,
+                                               uint64_t Npp_total, Philox& rng) {
+    Launched o;
+    o.ok = 0;
+    const int nl = S.nlambda;
+    V3<double> pos, dir;
+    if (phase == SKG_PHASE_STELLAR) {
+        double Lpp = S.Lv[ell] / (double)Npp_total;
+        if (!(Lpp > 0)) return o;
+        o.Lth = Lpp / S.min_weight_reduction;
+        int N = S.nstellar, h = 0;
+        double Lw = Lpp;
+        if (N > 1) {
+            double eb = S.emission_bias;
+            double X = rng.uniform();
+            if (X < eb) h = max(0, min(N - 1, (int)(N * X / eb)));
+            else h = dlocate_clip(S.Xvv + (size_t)ell * (N + 1), N + 1, (X - eb) / (1.0 - eb));
+            double Lh = S.starL[h * nl + ell];
+            if (!(Lh > 0)) return o;                         // launched with zero luminosity
+            Lw = Lpp * (1.0 / (1.0 - eb + eb * (S.Lv[ell] / N) / Lh));
+        }
+        pos = geom_position(S.stellar[h], rng);
+        dir = iso_direction(rng);
+        o.L = Lw; o.stellar = 1;
+    } else {
+        double Ltot = S.emit_Ltot[ell];
+        if (!(Ltot > 0)) return o;
+        double Lem = Ltot / (double)Npp_total;
+        o.Lth = Lem / S.min_weight_reduction;
+        const int nc = S.ncells;
+        const double* cdf = S.emit_cdf + (size_t)ell * (nc + 1);
+        double X = rng.uniform(), weight = 1.0;
+        int m;
+        if (phase == SKG_PHASE_DUST_SELFABS) m = dlocate_clip(cdf, nc + 1, X);
+        else {
+            double xi = S.dust_emission_bias;
+            if (X < xi) m = max(0, min(nc - 1, (int)(nc * X / xi)));
+            else m = dlocate_clip(cdf, nc + 1, (X - xi) / (1 - xi));
+            weight = 1.0 / (1 - xi + xi * (Ltot / nc) / S.emit_Lv[(size_t)ell * nc + m]);
+        }
+        o.L = Lem * weight;
+        if (!(o.L > 0)) return o;
+        pos = random_position_in_cell(g, m, rng);
+        dir = iso_direction(rng);
+        o.stellar = 0;
+    }
+    o.x = pos.x; o.y = pos.y; o.z = pos.z; o.kx = dir.x; o.ky = dir.y; o.kz = dir.z;
+    o.ok = 1;
+    return o;
+}
+
+// Peel-off weight toward a direction: the Henyey-Greenstein phase function value
+// (DustMix.cpp:648-654), weighted by kappa_sca*rho over the components (:319-331).  A negative
+// value aborts the peel-off.
+__device__ __noinline__ double peel_weight(const DevScene& S, int ell, int cell, double kx, double ky, double kz,
+                                           double gx_, double gy_, double gz_) {
+    const int nl = S.nlambda;
+    double cosalpha = kx * gx_ + ky * gy_ + kz * gz_;
+    if (S.ncomp == 1) {
+        double gg = S.asym[ell];
+        double t = 1.0 + gg * gg - 2 * gg * cosalpha;
+        return (1.0 - gg) * (1.0 + gg) / sqrt(t * t * t);
+    }
+    double sum = 0, acc = 0;
+    for (int h = 0; h < S.ncomp; h++) {
+        double wv = (cell >= 0) ? S.ksca[h * nl + ell] * S.rho[(size_t)h * S.ncells + cell] : 0.0;
+        double gg = S.asym[h * nl + ell];
+        double t = 1.0 + gg * gg - 2 * gg * cosalpha;
+        acc += wv * (1.0 - gg) * (1.0 + gg) / sqrt(t * t * t);
+        sum += wv;
+    }
+    return (sum > 0) ? acc / sum : -1.0;
+}
+
+// Forced interaction optical depth and weight: MonteCarloSimulation::simulatepropagation
+// (:513-531) with Random::exponcutoff (Random.cpp:163-176).  Returns tau; L is reweighted.
+__device__ __noinline__ double sample_interaction(double xi, double taupath, double& L, Philox& rng) {
+    auto expcut = [&](double xmax) -> double {
+        if (xmax < 1e-10) return rng.uniform() * xmax;
+        double x;
+        int guard = 0;
+        do { x = -log1p(-rng.uniform() * (-expm1(-xmax))); } while (x > xmax && ++guard < 64);
+        return fmin(x, xmax);
+    };
+    if (xi == 0.0) return expcut(taupath);
+    double X = rng.uniform();
+    double ti = (X < xi) ? rng.uniform() * taupath : expcut(taupath);
+    double p = -exp(-ti) / expm1(-taupath);
+    double q = (1.0 - xi) * p + xi / taupath;
+    L *= p / q;
+    return ti;
+}
+
+// New direction: DustSystem::randomMixForPosition (DustSystem.cpp:855-869) and the
+// Henyey-Greenstein sampling of DustMix::scatteringDirectionAndPolarization (DustMix.cpp:595-602).
+__device__ __noinline__ V3<double> scatter_direction(const DevScene& S, int ell, int cell, V3<double> k, Philox& rng) {
+    const int nl = S.nlambda;
+    int h = 0;
+    if (S.ncomp > 1 && cell >= 0) {
+        double tot = 0, pv[MAX_COMP];
+        for (int c = 0; c < S.ncomp; c++) { pv[c] = S.ksca[c * nl + ell] * S.rho[(size_t)c * S.ncells + cell]; tot += pv[c]; }
+        double X = rng.uniform(), acc = 0;
+        for (h = 0; h < S.ncomp - 1; h++) { acc += pv[h] / tot; if (X < acc) break; }
+    }
+    double gg = S.asym[h * nl + ell];
+    if (fabs(gg) < 1e-6) return iso_direction(rng);
+    double f = ((1.0 - gg) * (1.0 + gg)) / (1.0 - gg + 2.0 * gg * rng.uniform());
+    double costheta = (1.0 + gg * gg - f * f) / (2.0 * gg);
+    return rotate_direction(k, costheta, rng);
+}
+
+// finds the work item of global packet p (items sorted by begin; few items)
+SKG_D int find_item(const WorkItem* items, int n, uint64_t p) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (items[mid].begin <= p) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 template<typename R, template<typename> class Stepper>
-__global__ void __launch_bounds__(256)
-tracer_kernel(const DevGrid g, const DevScene* __restrict__ Sp, const RunParams P) {
-    const DevScene& S = *Sp;
-    __shared__ unsigned long long s_cnt[10];
-    if (threadIdx.x < 10) s_cnt[threadIdx.x] = 0;
+__global__ void __launch_bounds__(256, 3)
+tracer_kernel(const RunParams P) {
+    extern __shared__ unsigned char smem_raw[];
+    DevGrid* sg = reinterpret_cast<DevGrid*>(smem_raw);
+    __shared__ const DevScene* s_scene[MAX_SLOTS];
+    __shared__ unsigned long long s_cnt[C_N];
+    const BatchHeader H = *P.hdr;
+    for (int i = threadIdx.x; i < C_N; i += blockDim.x) s_cnt[i] = 0;
+    for (int i = threadIdx.x; i < H.nslots; i += blockDim.x) { sg[i] = P.grids[i]; s_scene[i] = P.scenes[i]; }
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
-    const uint64_t total = (uint64_t)P.nell * P.npp;
-    const int nl = S.nlambda;
-    const bool dust_phase = P.phase != SKG_PHASE_STELLAR;
-    const bool store = (P.phase == SKG_PHASE_STELLAR) ? (S.store_abs != 0) : (P.phase == SKG_PHASE_DUST_SELFABS);
-    double* labs = (P.phase == SKG_PHASE_STELLAR) ? S.labs_stel : S.labs_dust;
-    const bool peel_on = P.phase != SKG_PHASE_DUST_SELFABS;
+    const int phase = H.phase;
+    const bool peel_on = phase != SKG_PHASE_DUST_SELFABS;
 
     Philox rng;
+    int slot = 0;
     double L = 0, Lth = 0, Lpeel = 0, Lsca_acc = 0;
     int ell = 0, nscatt = 0, grp = 0;
     bool stellar = true, scat_peel = false;
@@ -108,14 +241,16 @@ tracer_kernel(const DevGrid g, const DevScene* __restrict__ Sp, const RunParams 
     int mode = M_FETCH, trav = T_NONE;
     int int_cell = -1;
     int pos_cell = -2;          // cell holding the packet position: -2 unknown, -1 outside the grid
+    uint64_t Npp_total = 1;
     double tau = 0, s = 0, tau_int = 0, s_int = 0;
     Stepper<R> st;
-    unsigned c_steps = 0, c_trav = 0, c_scatt = 0, c_peel = 0, c_abs = 0, c_pix = 0, c_nbr = 0, c_fb = 0,
-             c_err = 0, c_pk = 0;
+    unsigned c_steps = 0;
 
     while (true) {
         // ---------------- event processing: runs until a traversal starts or no work is left
         while (trav == T_NONE && mode != M_DONE) {
+            const DevGrid& g = sg[slot];
+            const DevScene& S = *s_scene[slot];
             switch (mode) {
             case M_FETCH: {
                 unsigned mask = __activemask();
@@ -124,60 +259,27 @@ tracer_kernel(const DevGrid g, const DevScene* __restrict__ Sp, const RunParams 
                 if (lane == leader) base = atomicAdd(P.work, (unsigned long long)__popc(mask));
                 base = __shfl_sync(mask, base, leader);
                 uint64_t p = base + __popc(mask & ((1u << lane) - 1));
-                if (p >= total) { mode = M_DONE; break; }
-                int ei = (int)(p / P.npp);
-                uint64_t ip = p - (uint64_t)ei * P.npp;
-                ell = P.ells[ei];
-                rng.init(P.seed, P.first_packet + ip, (uint32_t)ell | ((uint32_t)P.phase << 24));
-                c_pk++;
-                pos_cell = -2;
-                nscatt = 0;
-                V3<double> pos, dir;
-                if (!dust_phase) {
-                    // StellarSystem::launch (StellarSystem.cpp:116-158)
-                    double Lpp = S.Lv[ell] / (double)P.Npp_total;
-                    if (!(Lpp > 0)) break;                       // mode stays FETCH
-                    Lth = Lpp / S.min_weight_reduction;
-                    int N = S.nstellar, h = 0;
-                    double Lw = Lpp;
-                    if (N > 1) {
-                        double eb = S.emission_bias;
-                        double X = rng.uniform();
-                        if (X < eb) h = max(0, min(N - 1, (int)(N * X / eb)));
-                        else h = dlocate_clip(S.Xvv + (size_t)ell * (N + 1), N + 1, (X - eb) / (1.0 - eb));
-                        double Lh = S.starL[h * nl + ell];
-                        if (!(Lh > 0)) break;                    // launched with zero luminosity
-                        Lw = Lpp * (1.0 / (1.0 - eb + eb * (S.Lv[ell] / N) / Lh));
-                    }
-                    pos = geom_position(S.stellar[h], rng);      // GeometricStellarComp.cpp:75-81
-                    dir = iso_direction(rng);
-                    L = Lw; stellar = true;
-                } else {
-                    // PanMonteCarloSimulation.cpp:216-224 (self-absorption), :301-323 (emission)
-                    double Ltot = S.emit_Ltot[ell];
-                    if (!(Ltot > 0)) break;
-                    double Lem = Ltot / (double)P.Npp_total;
-                    Lth = Lem / S.min_weight_reduction;
-                    const int nc = S.ncells;
-                    const double* cdf = S.emit_cdf + (size_t)ell * (nc + 1);
-                    double X = rng.uniform(), weight = 1.0;
-                    int m;
-                    if (P.phase == SKG_PHASE_DUST_SELFABS) m = dlocate_clip(cdf, nc + 1, X);
-                    else {
-                        double xi = S.dust_emission_bias;
-                        if (X < xi) m = max(0, min(nc - 1, (int)(nc * X / xi)));
-                        else m = dlocate_clip(cdf, nc + 1, (X - xi) / (1 - xi));
-                        double Lmean = Ltot / nc;
-                        weight = 1.0 / (1 - xi + xi * Lmean / S.emit_Lv[(size_t)ell * nc + m]);
-                    }
-                    L = Lem * weight;
-                    if (!(L > 0)) break;
-                    pos = random_position_in_cell(g, m, rng);
-                    dir = iso_direction(rng);
-                    stellar = false;
-                }
-                r = mk3((R)pos.x, (R)pos.y, (R)pos.z);
-                k = mk3((R)dir.x, (R)dir.y, (R)dir.z);
+                if (p >= H.total) { mode = M_DONE; break; }
+                int it = find_item(P.items, H.nitems, p);
+                const WorkItem W = P.items[it];
+                uint64_t q = p - W.begin;
+                int ei = (int)(q / W.count);
+                uint64_t ip = W.first + (q - (uint64_t)ei * W.count);
+                slot = W.slot;
+                ell = P.ells[W.ell0 + ei];
+                Npp_total = W.npp_total;
+                rng.init(W.seed, ip, (uint32_t)ell | ((uint32_t)phase << 24));
+                atomicAdd(&s_cnt[C_PACKETS], 1ull);
+                mode = M_LAUNCH;        // the launch runs with the packet's own slot bound
+                break;
+            }
+            case M_LAUNCH: {
+                Launched o = launch_packet(g, S, phase, ell, Npp_total, rng);
+                if (!o.ok) { mode = M_FETCH; break; }
+                L = o.L; Lth = o.Lth; stellar = o.stellar;
+                r = mk3((R)o.x, (R)o.y, (R)o.z);
+                k = mk3((R)o.kx, (R)o.ky, (R)o.kz);
+                nscatt = 0; pos_cell = -2; int_cell = -1;
                 if (peel_on) { mode = M_PEEL_NEXT; grp = 0; scat_peel = false; }
                 else mode = M_MAIN1_START;
                 break;
@@ -187,24 +289,9 @@ tracer_kernel(const DevGrid g, const DevScene* __restrict__ Sp, const RunParams 
                 while (grp < S.ngroups) {
                     double w = 1.0;
                     if (scat_peel) {
-                        double gx_ = S.gkx[grp], gy_ = S.gky[grp], gz_ = S.gkz[grp];
-                        double cosalpha = (double)k.x * gx_ + (double)k.y * gy_ + (double)k.z * gz_;
-                        if (S.ncomp == 1) {                       // DustMix.cpp:648-654
-                            double gg = S.asym[ell];
-                            double t = 1.0 + gg * gg - 2 * gg * cosalpha;
-                            w = (1.0 - gg) * (1.0 + gg) / sqrt(t * t * t);
-                        } else {                                  // weights kappa_sca*rho (:319-331)
-                            double sum = 0, acc = 0;
-                            for (int h = 0; h < S.ncomp; h++) {
-                                double wv = (int_cell >= 0) ? S.ksca[h * nl + ell] * S.rho[(size_t)h * S.ncells + int_cell] : 0.0;
-                                double gg = S.asym[h * nl + ell];
-                                double t = 1.0 + gg * gg - 2 * gg * cosalpha;
-                                acc += wv * (1.0 - gg) * (1.0 + gg) / sqrt(t * t * t);
-                                sum += wv;
-                            }
-                            if (!(sum > 0)) { grp = S.ngroups; break; }   // abort peel-off
-                            w = acc / sum;
-                        }
+                        w = peel_weight(S, ell, int_cell, (double)k.x, (double)k.y, (double)k.z, S.gkx[grp], S.gky[grp],
+                                        S.gkz[grp]);
+                        if (w < 0) { grp = S.ngroups; break; }   // abort peel-off
                     }
                     Lpeel = L * w;
                     if (group_needs_traversal(S, grp, (double)r.x, (double)r.y, (double)r.z)) {
@@ -228,31 +315,16 @@ tracer_kernel(const DevGrid g, const DevScene* __restrict__ Sp, const RunParams 
             case M_AFTER_MAIN1: {
                 double taupath = tau;
                 if (taupath < 0.0 || isnan(taupath) || isinf(taupath)) {   // DustSystem.cpp:953-955
-                    atomicOr(P.err, ERR_NAN_TAU); c_err++; mode = M_FETCH; break;
+                    atomicOr(P.err, ERR_NAN_TAU); atomicAdd(&s_cnt[C_ERR], 1ull); mode = M_FETCH; break;
                 }
                 if (S.ncomp == 1) L = L * S.albedo[ell] * (-expm1(-taupath));   // :441-462
                 else L = Lsca_acc;
                 if (L <= 0 || (L <= Lth && nscatt >= S.min_scatt_events)) { mode = M_FETCH; break; }
-                if (nscatt >= P.max_scatt) { atomicOr(P.err, ERR_SCATT_BUDGET); c_err++; mode = M_FETCH; break; }
-                if (taupath == 0.0) { s_int = 0; int_cell = -1; mode = M_AFTER_MAIN2; break; }
-                // MonteCarloSimulation::simulatepropagation (:513-531), Random::exponcutoff (Random.cpp:163-176)
-                double xi = S.xi, ti;
-                auto expcut = [&](double xmax) -> double {
-                    if (xmax < 1e-10) return rng.uniform() * xmax;
-                    double x;
-                    int guard = 0;
-                    do { x = -log1p(-rng.uniform() * (-expm1(-xmax))); } while (x > xmax && ++guard < 64);
-                    return fmin(x, xmax);
-                };
-                if (xi == 0.0) ti = expcut(taupath);
-                else {
-                    double X = rng.uniform();
-                    ti = (X < xi) ? rng.uniform() * taupath : expcut(taupath);
-                    double p = -exp(-ti) / expm1(-taupath);
-                    double q = (1.0 - xi) * p + xi / taupath;
-                    L *= p / q;
+                if (nscatt >= P.max_scatt) {
+                    atomicOr(P.err, ERR_SCATT_BUDGET); atomicAdd(&s_cnt[C_ERR], 1ull); mode = M_FETCH; break;
                 }
-                tau_int = ti;
+                if (taupath == 0.0) { s_int = 0; mode = M_AFTER_MAIN2; break; }
+                tau_int = sample_interaction(S.xi, taupath, L, rng);
                 st.init(g, r.x, r.y, r.z, k.x, k.y, k.z, pos_cell);
                 trav = T_MAIN2; tau = 0; s = 0; s_int = -1; int_cell = -1;
                 break;
@@ -267,24 +339,10 @@ tracer_kernel(const DevGrid g, const DevScene* __restrict__ Sp, const RunParams 
                 break;
             }
             case M_SCATTER: {
-                // DustSystem::randomMixForPosition (DustSystem.cpp:855-869) + HG (DustMix.cpp:595-602)
-                int h = 0;
-                if (S.ncomp > 1 && int_cell >= 0) {
-                    double tot = 0, pv[MAX_COMP];
-                    for (int c = 0; c < S.ncomp; c++) { pv[c] = S.ksca[c * nl + ell] * S.rho[(size_t)c * S.ncells + int_cell]; tot += pv[c]; }
-                    double X = rng.uniform(), acc = 0;
-                    for (h = 0; h < S.ncomp - 1; h++) { acc += pv[h] / tot; if (X < acc) break; }
-                }
-                double gg = S.asym[h * nl + ell];
-                V3<double> kd = mk3((double)k.x, (double)k.y, (double)k.z), kn;
-                if (fabs(gg) < 1e-6) kn = iso_direction(rng);
-                else {
-                    double f = ((1.0 - gg) * (1.0 + gg)) / (1.0 - gg + 2.0 * gg * rng.uniform());
-                    double costheta = (1.0 + gg * gg - f * f) / (2.0 * gg);
-                    kn = rotate_direction(kd, costheta, rng);
-                }
+                V3<double> kn = scatter_direction(S, ell, int_cell, mk3((double)k.x, (double)k.y, (double)k.z), rng);
                 k = mk3((R)kn.x, (R)kn.y, (R)kn.z);
-                nscatt++; c_scatt++;
+                nscatt++;
+                atomicAdd(&s_cnt[C_SCATT], 1ull);
                 mode = M_MAIN1_START;
                 break;
             }
@@ -294,30 +352,40 @@ tracer_kernel(const DevGrid g, const DevScene* __restrict__ Sp, const RunParams 
         if (mode == M_DONE) break;
 
         // ---------------- one cell step of the current traversal
+        const DevGrid& g = sg[slot];
+        const DevScene& S = *s_scene[slot];
         int m; R ds;
         if (st.next(g, m, ds)) {
             c_steps++;
-            double dtau = kappa_rho<R>(S, m, ell) * (double)ds;
+            // one dust component: the FP32 tree walk carries the cell density in its leaf record
+            double kr = (S.ncomp == 1 && st.rho >= 0.f) ? S.kext[ell] * (double)st.rho : kappa_rho<R>(S, m, ell);
+            double dtau = kr * (double)ds;
             if (trav == T_PEEL) {
                 tau += dtau;
             } else if (trav == T_MAIN1) {
                 if (m >= 0) {
+                    const bool store = (phase == SKG_PHASE_STELLAR) ? (S.store_abs != 0) : (phase == SKG_PHASE_DUST_SELFABS);
                     if (S.ncomp == 1) {
                         if (store) {
                             double Lintm = L * exp(-tau) * (-expm1(-dtau));
-                            atomicAdd(labs + (size_t)m * nl + ell, (1.0 - S.albedo[ell]) * Lintm);
-                            c_abs++;
+                            double* labs = (phase == SKG_PHASE_STELLAR) ? S.labs_stel : S.labs_dust;
+                            atomicAdd(labs + (size_t)m * S.nlambda + ell, (1.0 - S.albedo[ell]) * Lintm);
+                            atomicAdd(&s_cnt[C_ABS], 1ull);
                         }
                     } else {
                         double ksca = 0, kext = 0;
                         for (int h = 0; h < S.ncomp; h++) {
                             double rh = rho_load<R>(S, (size_t)h * S.ncells + m);
-                            ksca += rh * S.ksca[h * nl + ell]; kext += rh * S.kext[h * nl + ell];
+                            ksca += rh * S.ksca[h * S.nlambda + ell]; kext += rh * S.kext[h * S.nlambda + ell];
                         }
                         double alb = (kext > 0.0) ? ksca / kext : 0.0;
                         double Lintm = L * exp(-tau) * (-expm1(-dtau));
                         Lsca_acc += alb * Lintm;
-                        if (store) { atomicAdd(labs + (size_t)m * nl + ell, (1.0 - alb) * Lintm); c_abs++; }
+                        if (store) {
+                            double* labs = (phase == SKG_PHASE_STELLAR) ? S.labs_stel : S.labs_dust;
+                            atomicAdd(labs + (size_t)m * S.nlambda + ell, (1.0 - alb) * Lintm);
+                            atomicAdd(&s_cnt[C_ABS], 1ull);
+                        }
                     }
                 }
                 tau += dtau;
@@ -326,19 +394,23 @@ tracer_kernel(const DevGrid g, const DevScene* __restrict__ Sp, const RunParams 
                 if (tn > tau_int) {
                     s_int = s + ((tau_int - tau) / (tn - tau)) * (sn - s);
                     int_cell = m;
-                    trav = T_NONE; mode = M_AFTER_MAIN2; c_trav++;
-                    c_nbr += st.scanned; c_fb += st.fallbacks;
+                    trav = T_NONE; mode = M_AFTER_MAIN2;
+                    atomicAdd(&s_cnt[C_TRAV], 1ull);
+                    atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.scanned);
+                    atomicAdd(&s_cnt[C_FB], (unsigned long long)st.fallbacks);
                 } else { tau = tn; s = sn; }
             }
         } else {
             // traversal ended
-            c_trav++;
-            c_nbr += st.scanned; c_fb += st.fallbacks;
-            if (st.steps > g.max_steps) { atomicOr(P.err, ERR_STEP_BUDGET); c_err++; }
+            atomicAdd(&s_cnt[C_TRAV], 1ull);
+            atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.scanned);
+            atomicAdd(&s_cnt[C_FB], (unsigned long long)st.fallbacks);
+            if (st.steps > g.max_steps) { atomicOr(P.err, ERR_STEP_BUDGET); atomicAdd(&s_cnt[C_ERR], 1ull); }
             if (trav == T_PEEL) {
-                detect_group(S, grp, ell, Lpeel, tau, scat_peel ? nscatt + 1 : 0, stellar,
-                             (double)r.x, (double)r.y, (double)r.z, c_pix);
-                c_peel++;
+                int adds = detect_group(S, grp, ell, Lpeel, tau, scat_peel ? nscatt + 1 : 0, stellar,
+                                        (double)r.x, (double)r.y, (double)r.z);
+                atomicAdd(&s_cnt[C_PIX], (unsigned long long)adds);
+                atomicAdd(&s_cnt[C_PEEL], 1ull);
                 grp++;
                 mode = M_PEEL_NEXT;
             } else if (trav == T_MAIN1) {
@@ -351,51 +423,42 @@ tracer_kernel(const DevGrid g, const DevScene* __restrict__ Sp, const RunParams 
         }
     }
 
-    atomicAdd(&s_cnt[0], (unsigned long long)c_pk);
-    atomicAdd(&s_cnt[1], (unsigned long long)c_steps);
-    atomicAdd(&s_cnt[2], (unsigned long long)c_trav);
-    atomicAdd(&s_cnt[3], (unsigned long long)c_scatt);
-    atomicAdd(&s_cnt[4], (unsigned long long)c_peel);
-    atomicAdd(&s_cnt[5], (unsigned long long)c_abs);
-    atomicAdd(&s_cnt[6], (unsigned long long)c_pix);
-    atomicAdd(&s_cnt[7], (unsigned long long)c_nbr);
-    atomicAdd(&s_cnt[8], (unsigned long long)c_fb);
-    atomicAdd(&s_cnt[9], (unsigned long long)c_err);
+    atomicAdd(&s_cnt[C_STEPS], (unsigned long long)c_steps);
     __syncthreads();
-    if (threadIdx.x < 10) atomicAdd(P.counters + threadIdx.x, s_cnt[threadIdx.x]);
+    if (threadIdx.x < C_N) atomicAdd(P.counters + threadIdx.x, s_cnt[threadIdx.x]);
 }
 
 // ---------------------------------------------------------------------------------------------
 template<typename R, template<typename> class Stepper>
-static cudaError_t launch_one(const DevGrid& g, const DevScene* dS, const RunParams& P, int blocks,
-                              int threads, cudaStream_t stream) {
+static cudaError_t launch_one(const RunParams& P, int nslots, int blocks, int threads, cudaStream_t stream) {
     auto kern = tracer_kernel<R, Stepper>;
+    size_t smem = (size_t)nslots * sizeof(DevGrid);
     if (blocks <= 0) {
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem);
         blocks = sms * (per > 0 ? per : 1);
     }
-    kern<<<blocks, threads, 0, stream>>>(g, dS, P);
+    kern<<<blocks, threads, smem, stream>>>(P);
     return cudaGetLastError();
 }
 
-cudaError_t launch_tracer(const DevGrid& g, const DevScene* dS, const RunParams& P, int precision,
-                          int blocks, int threads, cudaStream_t stream) {
+cudaError_t launch_tracer(int grid_type, const RunParams& P, int nslots, int precision, int blocks, int threads,
+                          cudaStream_t stream) {
     if (threads <= 0) threads = 256;
     bool f64 = precision == SKG_PREC_FP64;
-    switch (g.type) {
+    switch (grid_type) {
     case SKG_GRID_CARTESIAN:
-        return f64 ? launch_one<double, CartStepper>(g, dS, P, blocks, threads, stream)
-                   : launch_one<float, CartStepper>(g, dS, P, blocks, threads, stream);
+        return f64 ? launch_one<double, CartStepper>(P, nslots, blocks, threads, stream)
+                   : launch_one<float, CartStepper>(P, nslots, blocks, threads, stream);
     case SKG_GRID_OCTREE:
     case SKG_GRID_BINTREE:
-        return f64 ? launch_one<double, TreeStepper>(g, dS, P, blocks, threads, stream)
-                   : launch_one<float, TreeStepper>(g, dS, P, blocks, threads, stream);
+        return f64 ? launch_one<double, TreeStepper>(P, nslots, blocks, threads, stream)
+                   : launch_one<float, TreeStepper>(P, nslots, blocks, threads, stream);
     default:
-        return f64 ? launch_one<double, VoronoiStepper>(g, dS, P, blocks, threads, stream)
-                   : launch_one<float, VoronoiStepper>(g, dS, P, blocks, threads, stream);
+        return f64 ? launch_one<double, VoronoiStepper>(P, nslots, blocks, threads, stream)
+                   : launch_one<float, VoronoiStepper>(P, nslots, blocks, threads, stream);
     }
 }
 

@@ -2,6 +2,7 @@
 // numbers and per-wall neighbour lists) and its flat arrays for the device.
 #pragma once
 #include "../../include/skirt_b200.h"
+#include <vector_types.h>
 #include <cstdint>
 #include <functional>
 #include <vector>
@@ -44,6 +45,20 @@ struct Tree {
                                         std::vector<double>&)>& sample);
     void build_from_splits(const uint8_t* split, int64_t nsplit);
 };
+
+// Rope-linked tree for the FP32 production walk (see build_rope_tree in skg_host.cpp).
+//   lrec: 4 float4 per leaf, leaves in depth-first order
+//     [0] = (xmin, ymin, zmin, density placeholder)   [1] = (xmax, ymax, zmax, int cell number)
+//     [2] = int ropes of walls 0..3                   [3] = int ropes of walls 4,5, 0, 0
+//   irec: 3 float4 per internal node: (split x, y, z, int split direction or -1 for an octree node),
+//         then 8 int child references
+//   references: >= 0 leaf index, -1 none (outside the domain), <= -2 internal node -(ref + 2)
+struct RopeTree {
+    std::vector<float4> lrec, irec;
+    std::vector<int> cell_leaf;
+    int root_ref = -1;
+};
+void build_rope_tree(const skg_grid& g, RopeTree& out);
 
 }  // namespace skg
 

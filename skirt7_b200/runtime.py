@@ -156,6 +156,54 @@ class Context:
         self._ck(self.lib.skg_reset_dust_absorption(self.h))
 
 
+class Batch:
+    """Staging for launches that carry slices of several simulations at once (skg_batch)."""
+
+    def __init__(self, device=0, max_slots=64, max_items=256, max_ells=1024):
+        self.lib = A.load()
+        h = C.c_void_p()
+        A.check(self.lib.skg_batch_create(device, max_slots, max_items, max_ells, C.byref(h)))
+        self.h = h
+        self._keep = []
+
+    def run(self, phase, slices, precision=A.PREC_FP32, graph=False, stream=None, max_scatt=0):
+        """slices: list of (Context, ells, npp, first, count, seed)."""
+        n = len(slices)
+        arr = (A.Work * max(n, 1))()
+        keep = []
+        for i, (ctx, ells, npp, first, count, seed) in enumerate(slices):
+            e = np.ascontiguousarray(ells, dtype=np.int32)
+            keep.append(e)
+            arr[i] = A.Work(ctx.h.value, e.ctypes.data_as(A.i32p), len(e), int(npp), int(first), int(count), int(seed))
+        opts = A.RunOpts(precision, 0, max_scatt, 0, 0, 1)
+        A.check(self.lib.skg_batch_run(self.h, phase, arr, n, C.byref(opts), A.BATCH_GRAPH if graph else 0, stream))
+        self._keep = keep
+
+    def sync(self, timeout_ms=-1):
+        A.check(self.lib.skg_batch_sync(self.h, timeout_ms))
+
+    def last_ms(self):
+        ms = C.c_float()
+        A.check(self.lib.skg_batch_last_ms(self.h, C.byref(ms)))
+        return ms.value
+
+    def counters(self):
+        c = A.Counters()
+        self.lib.skg_batch_counters(self.h, C.byref(c))
+        return {n: getattr(c, n) for n, _ in A.Counters._fields_}
+
+    def close(self):
+        if self.h:
+            self.lib.skg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # --------------------------------------------------------------------------------------------
 # grid builders
 

@@ -69,4 +69,5 @@ def test_dust_emission_matches_oracle(orc):
         z, ok = zscores([f(g) for g in G], [f(o) for o in O])
         mean = np.mean([f(o) for o in O], 0)
         ok &= mean > 2e-3 * mean.sum()
-        assert np.max(np.abs(z[ok])) < 5.0 and np.mean(np.abs(z[ok]) > 3) < 0.05, (ell, np.sort(np.abs(z[ok]))[-5:])
+        zz = np.abs(z[ok])
+        assert zz.max() < 5.0 and np.sum(zz > 3) <= max(1, 0.05 * zz.size), (ell, np.sort(zz)[-5:])
