@@ -711,7 +711,7 @@ int skg_run_phase(skg_ctx* ctx, int phase, const int32_t* ells, int nell, uint64
         int precision = opts ? opts->precision : SKG_PREC_FP32;
         int blocks = opts ? opts->blocks : 0, threads = opts ? opts->threads : 0;
         CK(cudaEventRecord(ctx->ev0, s));
-        CK(launch_tracer(ctx->grid.type, P, 1, precision, blocks, threads, s));
+        CK(launch_tracer(ctx->grid.type, ctx->grid.search == SKG_SEARCH_BOOKKEEPING, P, 1, precision, blocks, threads, s));
         CK(cudaEventRecord(ctx->ev1, s));
         return SKG_OK;
     } catch (const Failure& f) { return fail(ctx, f); }
@@ -981,7 +981,7 @@ struct skg_batch {
     int* h_ells = nullptr;
     cudaEvent_t copied = nullptr;          // the previous launch's tables have been read
     cudaGraphExec_t graph = nullptr;
-    int g_type = -1, g_prec = -1, g_blocks = -1, g_threads = -1;
+    int g_type = -1, g_bk = -1, g_prec = -1, g_blocks = -1, g_threads = -1;
     cudaStream_t g_stream = nullptr;
     std::string error;
 };
@@ -1057,7 +1057,7 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
         cudaStream_t s = stream ? (cudaStream_t)stream : b->stream;
         // the pinned tables may still be read by the previous launch's copies
         CK(cudaEventSynchronize(b->copied));
-        int nslots = 0, nells = 0, gtype = -1;
+        int nslots = 0, nells = 0, gtype = -1, gbk = -1;
         uint64_t total = 0;
         std::vector<skg_ctx*> slots;
         for (int i = 0; i < nwork; i++) {
@@ -1069,6 +1069,9 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
             auto tree = [](int t) { return t == SKG_GRID_OCTREE || t == SKG_GRID_BINTREE; };
             REQUIRE(w.ctx->grid.type == gtype || (tree(gtype) && tree(w.ctx->grid.type)),
                     "a batch holds one kind of grid");
+            const int bk = tree(gtype) && w.ctx->grid.search == SKG_SEARCH_BOOKKEEPING;
+            if (gbk < 0) gbk = bk;
+            REQUIRE(bk == gbk, "a batch holds trees of one search method kind (Bookkeeping or not)");
             if (phase != SKG_PHASE_STELLAR) REQUIRE(w.ctx->emit_cdf != nullptr, "dust phases need dust emission enabled");
             int slot = -1;
             for (int q = 0; q < nslots; q++) if (slots[q] == w.ctx) slot = q;
@@ -1113,11 +1116,12 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
             CK(cudaMemsetAsync(T.work, 0, sizeof(unsigned long long), q));
             CK(cudaMemsetAsync(T.err, 0, sizeof(unsigned), q));
             // every slot's DevGrid is copied into shared memory: size for the batch's capacity
-            CK(launch_tracer(gtype < 0 ? SKG_GRID_CARTESIAN : gtype, P, T.max_slots, precision, blocks, threads, q));
+            CK(launch_tracer(gtype < 0 ? SKG_GRID_CARTESIAN : gtype, gbk == 1, P, T.max_slots, precision, blocks,
+                             threads, q));
         };
         CK(cudaEventRecord(b->ev0, s));
         if (flags & SKG_BATCH_GRAPH) {
-            bool same = b->graph && b->g_type == gtype && b->g_prec == precision && b->g_blocks == blocks &&
+            bool same = b->graph && b->g_type == gtype && b->g_bk == gbk && b->g_prec == precision && b->g_blocks == blocks &&
                         b->g_threads == threads;
             if (!same) {
                 if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
@@ -1129,7 +1133,7 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
                 cudaError_t e = cudaGraphInstantiate(&b->graph, gr, 0);
                 cudaGraphDestroy(gr);
                 CK(e);
-                b->g_type = gtype; b->g_prec = precision; b->g_blocks = blocks; b->g_threads = threads;
+                b->g_type = gtype; b->g_bk = gbk; b->g_prec = precision; b->g_blocks = blocks; b->g_threads = threads;
             }
             CK(cudaGraphLaunch(b->graph, s));
         } else {
@@ -1178,5 +1182,6 @@ int skg_batch_last_ms(skg_batch* b, float* ms) {
     cudaEventElapsedTime(ms, b->ev0, b->ev1);
     return SKG_OK;
 }
+
 
 }  // extern "C"

@@ -19,8 +19,8 @@ struct Philox {
     uint32_t key0, key1;      // seed
     uint32_t c1, c2, c3;      // packet id / stream words
     uint32_t c0;              // draw block counter
-    uint32_t buf[4];
-    int      left;            // unread words in buf
+    uint32_t b0, b1, b2, b3;  // the current block (named, not an array: stays in registers)
+    int      left;            // unread words of the block
 
     SKG_D void init(uint64_t seed, uint64_t packet, uint32_t stream) {
         key0 = (uint32_t)seed; key1 = (uint32_t)(seed >> 32);
@@ -38,13 +38,14 @@ struct Philox {
             x0 = y0; x1 = y1; x2 = y2; x3 = y3;
             k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
         }
-        buf[0] = x0; buf[1] = x1; buf[2] = x2; buf[3] = x3;
+        b0 = x0; b1 = x1; b2 = x2; b3 = x3;
         left = 4;
         c0++;
     }
     SKG_D uint32_t next32() {
         if (left == 0) refill();
-        return buf[4 - (left--)];
+        const int i = 4 - (left--);
+        return (i == 0) ? b0 : (i == 1) ? b1 : (i == 2) ? b2 : b3;
     }
     // uniform deviate in the open interval (0,1) with 2^-32 resolution (the reference's MT19937
     // deviates also exclude 0 and 1, Random.cpp:125)

@@ -97,38 +97,52 @@ SKG_D int locate_clip_dev(const DevGrid& g, int n /* planes */, R x) {
     return jl;
 }
 
+// The (at most three) entry segments outside the grid (m = -1) that a path starts with.  Three
+// named slots instead of an array: an indexed array would put the whole stepper in local memory.
+template<typename R> struct Pend {
+    R a, b, c;
+    int n, i;
+    SKG_D void clear() { n = 0; i = 0; }
+    SKG_D void push(R ds) { if (n == 0) a = ds; else if (n == 1) b = ds; else c = ds; n++; }
+    SKG_D bool pop(R& ds) {
+        if (i >= n) return false;
+        ds = (i == 0) ? a : (i == 1) ? b : c;
+        i++;
+        return true;
+    }
+};
+
 // DustGridPath::moveInside (DustGridPath.cpp:57-150).  Returns false for OUTSIDE; entry
-// segments (m = -1) are appended to pend[] when their ds > 0.
+// segments (m = -1) are appended to pd when their ds > 0.
 template<typename R>
-SKG_D bool move_inside(const DevGrid& g, R eps, R& rx, R& ry, R& rz, R kx, R ky, R kz,
-                       R* pend, int& npend) {
+SKG_D bool move_inside(const DevGrid& g, R eps, R& rx, R& ry, R& rz, R kx, R ky, R kz, Pend<R>& pd) {
     const R xmin = (R)g.xmin, xmax = (R)g.xmax, ymin = (R)g.ymin, ymax = (R)g.ymax,
             zmin = (R)g.zmin, zmax = (R)g.zmax;
     if (rx <= xmin) {
         if (kx <= (R)0) return false;
-        R ds = (xmin - rx) / kx; if (ds > (R)0) pend[npend++] = ds;
+        R ds = (xmin - rx) / kx; if (ds > (R)0) pd.push(ds);
         rx = xmin + eps; ry += ky * ds; rz += kz * ds;
     } else if (rx >= xmax) {
         if (kx >= (R)0) return false;
-        R ds = (xmax - rx) / kx; if (ds > (R)0) pend[npend++] = ds;
+        R ds = (xmax - rx) / kx; if (ds > (R)0) pd.push(ds);
         rx = xmax - eps; ry += ky * ds; rz += kz * ds;
     }
     if (ry <= ymin) {
         if (ky <= (R)0) return false;
-        R ds = (ymin - ry) / ky; if (ds > (R)0) pend[npend++] = ds;
+        R ds = (ymin - ry) / ky; if (ds > (R)0) pd.push(ds);
         rx += kx * ds; ry = ymin + eps; rz += kz * ds;
     } else if (ry >= ymax) {
         if (ky >= (R)0) return false;
-        R ds = (ymax - ry) / ky; if (ds > (R)0) pend[npend++] = ds;
+        R ds = (ymax - ry) / ky; if (ds > (R)0) pd.push(ds);
         rx += kx * ds; ry = ymax - eps; rz += kz * ds;
     }
     if (rz <= zmin) {
         if (kz <= (R)0) return false;
-        R ds = (zmin - rz) / kz; if (ds > (R)0) pend[npend++] = ds;
+        R ds = (zmin - rz) / kz; if (ds > (R)0) pd.push(ds);
         rx += kx * ds; ry += ky * ds; rz = zmin + eps;
     } else if (rz >= zmax) {
         if (kz >= (R)0) return false;
-        R ds = (zmax - rz) / kz; if (ds > (R)0) pend[npend++] = ds;
+        R ds = (zmax - rz) / kz; if (ds > (R)0) pd.push(ds);
         rx += kx * ds; ry += ky * ds; rz = zmax - eps;
     }
     return true;
@@ -140,7 +154,7 @@ template<typename R>
 struct CartStepper {
     R x, y, z, kx, ky, kz;
     int i, j, k;
-    R pend[3]; int npend, ipend;
+    Pend<R> pd;
     bool done;
     int steps;
     int cell0;                  // cell holding the start position (-1 if it lies outside the grid)
@@ -150,7 +164,7 @@ struct CartStepper {
     // hint: a cell known to hold the start position (or -1); it is verified against the planes
     SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz, int hint = -1) {
         x = rx; y = ry; z = rz; kx = dx; ky = dy; kz = dz;
-        npend = 0; ipend = 0; done = false; steps = 0; cell0 = -1;
+        pd.clear(); done = false; steps = 0; cell0 = -1;
         const R xmin = (R)g.xmin, xmax = (R)g.xmax, ymin = (R)g.ymin, ymax = (R)g.ymax,
                 zmin = (R)g.zmin, zmax = (R)g.zmax;
         if (hint >= 0) {
@@ -164,42 +178,42 @@ struct CartStepper {
         R ds;
         // entry into the box (CartesianDustGrid.cpp:151-222); "return path->clear()" empties the path
         if (x < xmin) {
-            if (kx <= (R)0) { done = true; npend = 0; return; }
-            ds = (xmin - x) / kx; if (ds > (R)0) pend[npend++] = ds;
+            if (kx <= (R)0) { done = true; pd.n = 0; return; }
+            ds = (xmin - x) / kx; if (ds > (R)0) pd.push(ds);
             x = xmin + (R)1e-8 * (gx<R>(g, 1) - gx<R>(g, 0)); y += ky * ds; z += kz * ds;
         } else if (x > xmax) {
-            if (kx >= (R)0) { done = true; npend = 0; return; }
-            ds = (xmax - x) / kx; if (ds > (R)0) pend[npend++] = ds;
+            if (kx >= (R)0) { done = true; pd.n = 0; return; }
+            ds = (xmax - x) / kx; if (ds > (R)0) pd.push(ds);
             x = xmax - (R)1e-8 * (gx<R>(g, g.nx) - gx<R>(g, g.nx - 1)); y += ky * ds; z += kz * ds;
         }
         if (y < ymin) {
-            if (ky <= (R)0) { done = true; npend = 0; return; }
-            ds = (ymin - y) / ky; if (ds > (R)0) pend[npend++] = ds;
+            if (ky <= (R)0) { done = true; pd.n = 0; return; }
+            ds = (ymin - y) / ky; if (ds > (R)0) pd.push(ds);
             x += kx * ds; y = ymin + (R)1e-8 * (gy<R>(g, 1) - gy<R>(g, 0)); z += kz * ds;
         } else if (y > ymax) {
-            if (ky >= (R)0) { done = true; npend = 0; return; }
-            ds = (ymax - y) / ky; if (ds > (R)0) pend[npend++] = ds;
+            if (ky >= (R)0) { done = true; pd.n = 0; return; }
+            ds = (ymax - y) / ky; if (ds > (R)0) pd.push(ds);
             x += kx * ds; y = ymax - (R)1e-8 * (gy<R>(g, g.ny) - gy<R>(g, g.ny - 1)); z += kz * ds;
         }
         if (z < zmin) {
-            if (kz <= (R)0) { done = true; npend = 0; return; }
-            ds = (zmin - z) / kz; if (ds > (R)0) pend[npend++] = ds;
+            if (kz <= (R)0) { done = true; pd.n = 0; return; }
+            ds = (zmin - z) / kz; if (ds > (R)0) pd.push(ds);
             x += kx * ds; y += ky * ds; z = zmin + (R)1e-8 * (gz<R>(g, 1) - gz<R>(g, 0));
         } else if (z > zmax) {
-            if (kz >= (R)0) { done = true; npend = 0; return; }
-            ds = (zmax - z) / kz; if (ds > (R)0) pend[npend++] = ds;
+            if (kz >= (R)0) { done = true; pd.n = 0; return; }
+            ds = (zmax - z) / kz; if (ds > (R)0) pd.push(ds);
             x += kx * ds; y += ky * ds; z = zmax - (R)1e-8 * (gz<R>(g, g.nz) - gz<R>(g, g.nz - 1));
         }
-        if (x < xmin || x > xmax || y < ymin || y > ymax || z < zmin || z > zmax) { done = true; npend = 0; return; }
+        if (x < xmin || x > xmax || y < ymin || y > ymax || z < zmin || z > zmax) { done = true; pd.n = 0; return; }
         i = locate_clip_dev<R, gx<R>>(g, g.nx + 1, x);
         j = locate_clip_dev<R, gy<R>>(g, g.ny + 1, y);
         k = locate_clip_dev<R, gz<R>>(g, g.nz + 1, z);
-        if (npend == 0) cell0 = k + g.nz * j + g.nz * g.ny * i;
+        if (pd.n == 0) cell0 = k + g.nz * j + g.nz * g.ny * i;
     }
 
     // next segment; false when the path has ended
     SKG_D bool next(const DevGrid& g, int& m, R& ds) {
-        if (ipend < npend) { m = -1; ds = pend[ipend++]; return true; }
+        if (pd.pop(ds)) { m = -1; return true; }
         while (!done) {
             if (++steps > g.max_steps) { done = true; return false; }
             m = k + g.nz * j + g.nz * g.ny * i;
@@ -280,7 +294,7 @@ template<typename R>
 struct TreeNodeWalk {
     R x, y, z, kx, ky, kz;
     int node;
-    R pend[3]; int npend, ipend;
+    Pend<R> pd;
     bool done;
     int steps;
     int fallbacks;
@@ -289,7 +303,7 @@ struct TreeNodeWalk {
     static constexpr float rho = -1.f;
 
     SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz, int hint = -1) {
-        kx = dx; ky = dy; kz = dz; npend = 0; ipend = 0; done = false; steps = 0; fallbacks = 0; scanned = 0;
+        kx = dx; ky = dy; kz = dz; pd.clear(); done = false; steps = 0; fallbacks = 0; scanned = 0;
         cell0 = -1;
         if (hint >= 0) {
             int l = g.cell_node[hint];
@@ -297,15 +311,15 @@ struct TreeNodeWalk {
             if (box_contains(lo, hi, rx, ry, rz)) { node = l; x = rx; y = ry; z = rz; cell0 = hint; return; }
         }
         R eps = PT<R>::eps(g);
-        bool ok = move_inside<R>(g, eps, rx, ry, rz, kx, ky, kz, pend, npend);
+        bool ok = move_inside<R>(g, eps, rx, ry, rz, kx, ky, kz, pd);
         node = ok ? tree_whichnode<R>(g, rx, ry, rz) : -1;
-        if (node < 0) { npend = 0; done = true; return; }   // path->clear()
-        if (npend == 0) cell0 = g.node_cell[node];
+        if (node < 0) { pd.n = 0; done = true; return; }   // path->clear()
+        if (pd.n == 0) cell0 = g.node_cell[node];
         x = rx; y = ry; z = rz;
     }
 
     SKG_D bool next(const DevGrid& g, int& m, R& ds) {
-        if (ipend < npend) { m = -1; ds = pend[ipend++]; return true; }
+        if (pd.pop(ds)) { m = -1; return true; }
         while (!done) {
             if (++steps > g.max_steps) { done = true; return false; }
             if (g.search == 2) { if (bookkeeping(g, m, ds)) return true; else continue; }
@@ -424,10 +438,11 @@ struct TreeNodeWalk {
     }
 };
 
-// FP32 production walk of the tree with the Neighbor search (TreeDustGrid.cpp:443-497): the
-// current leaf's 32-byte record stays in registers, so a step costs two dependent loads -- the
-// neighbour ids of the exit wall and the candidate's record, which becomes the next current one.
-// TopDown and Bookkeeping run through the node-based walk above.
+// FP32 production walk of the tree (the cells of TreeDustGrid.cpp:443-497, Neighbor or TopDown
+// search): the current leaf's 64-byte record stays in registers; a step follows the rope of the
+// exit wall and descends from it through the internal records to the leaf holding the new point,
+// whose record becomes the current one.  FP64 walks and the Bookkeeping search run through the
+// node-based walk above (the launchers pick TreeNodeWalk<float> for Bookkeeping).
 template<typename R> struct TreeStepper : TreeNodeWalk<R> {};
 
 template<>
@@ -435,12 +450,11 @@ struct TreeStepper<float> {
     float x, y, z, kx, ky, kz;
     float4 r0, r1, r2, r3;      // the current leaf's record
     int leaf;
-    float pend[3]; int npend, ipend;
+    Pend<float> pd;
     bool done;
     int steps, fallbacks, scanned;
     int cell0;
     float rho;                  // density embedded in the record of the last segment's cell
-    TreeNodeWalk<float> bk;     // Bookkeeping search (octree index arithmetic)
 
     SKG_D void load(const DevGrid& g, int li) {
         const float4* p = g.lrec + 4 * (size_t)li;
@@ -472,33 +486,23 @@ struct TreeStepper<float> {
     }
 
     SKG_D void init(const DevGrid& g, float rx, float ry, float rz, float dx, float dy, float dz, int hint = -1) {
-        kx = dx; ky = dy; kz = dz; npend = 0; ipend = 0; done = false; steps = 0; fallbacks = 0; scanned = 0;
+        kx = dx; ky = dy; kz = dz; pd.clear(); done = false; steps = 0; fallbacks = 0; scanned = 0;
         cell0 = -1; rho = -1.f;
-        if (g.search == SKG_SEARCH_BOOKKEEPING) {
-            bk.init(g, rx, ry, rz, dx, dy, dz, hint);
-            cell0 = bk.cell0; done = bk.done;
-            return;
-        }
         if (hint >= 0) {
             leaf = __ldg(g.cell_leaf + hint);
             load(g, leaf);
             if (inside(rx, ry, rz)) { cell0 = hint; x = rx; y = ry; z = rz; return; }
         }
-        bool ok = move_inside<float>(g, g.epsf, rx, ry, rz, kx, ky, kz, pend, npend);
+        bool ok = move_inside<float>(g, g.epsf, rx, ry, rz, kx, ky, kz, pd);
         leaf = ok ? locate(g, rx, ry, rz) : -1;
-        if (leaf < 0) { npend = 0; done = true; return; }
+        if (leaf < 0) { pd.n = 0; done = true; return; }
         load(g, leaf);
-        if (npend == 0) cell0 = __float_as_int(r1.w);
+        if (pd.n == 0) cell0 = __float_as_int(r1.w);
         x = rx; y = ry; z = rz;
     }
 
     SKG_D bool next(const DevGrid& g, int& m, float& ds) {
-        if (g.search == SKG_SEARCH_BOOKKEEPING) {
-            bool r = bk.next(g, m, ds);
-            steps = bk.steps; done = bk.done;
-            return r;
-        }
-        if (ipend < npend) { m = -1; ds = pend[ipend++]; rho = 0.f; return true; }
+        if (pd.pop(ds)) { m = -1; rho = 0.f; return true; }
         const float eps = g.epsf;
         while (!done) {
             if (++steps > g.max_steps) { done = true; return false; }
@@ -584,7 +588,7 @@ template<typename R>
 struct VoronoiStepper {
     R x, y, z, kx, ky, kz;
     int mr;
-    R pend[3]; int npend, ipend;
+    Pend<R> pd;
     bool done;
     int steps;
     int fallbacks;
@@ -595,7 +599,7 @@ struct VoronoiStepper {
     // hint: the cell holding the start position (the interaction point lies in the cell of its
     // segment); accepted for a position strictly inside the domain
     SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz, int hint = -1) {
-        kx = dx; ky = dy; kz = dz; npend = 0; ipend = 0; done = false; steps = 0; fallbacks = 0; scanned = 0;
+        kx = dx; ky = dy; kz = dz; pd.clear(); done = false; steps = 0; fallbacks = 0; scanned = 0;
         cell0 = -1;
         if (hint >= 0 && rx > (R)g.xmin && rx < (R)g.xmax && ry > (R)g.ymin && ry < (R)g.ymax &&
             rz > (R)g.zmin && rz < (R)g.zmax) {
@@ -603,11 +607,11 @@ struct VoronoiStepper {
             return;
         }
         R eps = PT<R>::eps(g);
-        bool ok = move_inside<R>(g, eps, rx, ry, rz, kx, ky, kz, pend, npend);
+        bool ok = move_inside<R>(g, eps, rx, ry, rz, kx, ky, kz, pd);
         if (!ok) { rx = ry = rz = (R)INFINITY; }
         mr = voronoi_cell_index<R>(g, rx, ry, rz);
-        if (mr < 0) { npend = 0; done = true; return; }
-        if (npend == 0) cell0 = mr;
+        if (mr < 0) { pd.n = 0; done = true; return; }
+        if (pd.n == 0) cell0 = mr;
         x = rx; y = ry; z = rz;
     }
 
@@ -617,7 +621,7 @@ struct VoronoiStepper {
 // FP64: the reference arithmetic on the generator sites (VoronoiMesh.cpp:803-858)
 template<>
 SKG_D bool VoronoiStepper<double>::next(const DevGrid& g, int& m, double& ds) {
-    if (ipend < npend) { m = -1; ds = pend[ipend++]; return true; }
+    if (pd.pop(ds)) { m = -1; return true; }
     while (!done) {
         if (++steps > g.max_steps) { done = true; return false; }
         V3<double> pr = site_pos<double>(g, mr);
@@ -667,7 +671,7 @@ SKG_D bool VoronoiStepper<double>::next(const DevGrid& g, int& m, double& ds) {
 // FP32: precomputed bisector planes, one 16-byte load per neighbour entry
 template<>
 SKG_D bool VoronoiStepper<float>::next(const DevGrid& g, int& m, float& ds) {
-    if (ipend < npend) { m = -1; ds = pend[ipend++]; return true; }
+    if (pd.pop(ds)) { m = -1; return true; }
     while (!done) {
         if (++steps > g.max_steps) { done = true; return false; }
         float sq = FLT_MAX;

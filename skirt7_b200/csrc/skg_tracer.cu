@@ -25,6 +25,13 @@
 
 namespace skg {
 
+#ifndef SKG_EVENT_LANES
+#define SKG_EVENT_LANES 32
+#endif
+#ifndef SKG_TRACER_MIN_BLOCKS
+#define SKG_TRACER_MIN_BLOCKS 3
+#endif
+
 enum Mode : int { M_FETCH = 0, M_LAUNCH, M_PEEL_NEXT, M_MAIN1_START, M_AFTER_MAIN1, M_AFTER_MAIN2, M_SCATTER, M_DONE };
 enum Trav : int { T_NONE = 0, T_PEEL, T_MAIN1, T_MAIN2 };
 enum Cnt : int { C_PACKETS = 0, C_STEPS, C_TRAV, C_SCATT, C_PEEL, C_ABS, C_PIX, C_NBR, C_FB, C_ERR, C_N };
@@ -217,7 +224,7 @@ SKG_D int find_item(const WorkItem* items, int n, uint64_t p) {
 }
 
 template<typename R, template<typename> class Stepper>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, SKG_TRACER_MIN_BLOCKS)
 tracer_kernel(const RunParams P) {
     extern __shared__ unsigned char smem_raw[];
     DevGrid* sg = reinterpret_cast<DevGrid*>(smem_raw);
@@ -247,8 +254,14 @@ tracer_kernel(const RunParams P) {
     unsigned c_steps = 0;
 
     while (true) {
-        // ---------------- event processing: runs until a traversal starts or no work is left
-        while (trav == T_NONE && mode != M_DONE) {
+        // ---------------- event processing: runs until a traversal starts or no work is left.
+        // A lane whose traversal ended waits (idle in the step below) until SKG_EVENT_LANES lanes
+        // of the warp, or all of its live lanes, are waiting, so that the divergent event code is
+        // paid once for many lanes instead of once per finished traversal.
+        const unsigned live = __activemask();
+        const unsigned waiting = __ballot_sync(live, trav == T_NONE);
+        const bool run_events = __popc(waiting) >= SKG_EVENT_LANES || waiting == live;
+        while (run_events && trav == T_NONE && mode != M_DONE) {
             const DevGrid& g = sg[slot];
             const DevScene& S = *s_scene[slot];
             switch (mode) {
@@ -350,6 +363,7 @@ tracer_kernel(const RunParams P) {
             }
         }
         if (mode == M_DONE) break;
+        if (trav == T_NONE) continue;
 
         // ---------------- one cell step of the current traversal
         const DevGrid& g = sg[slot];
@@ -444,8 +458,8 @@ static cudaError_t launch_one(const RunParams& P, int nslots, int blocks, int th
     return cudaGetLastError();
 }
 
-cudaError_t launch_tracer(int grid_type, const RunParams& P, int nslots, int precision, int blocks, int threads,
-                          cudaStream_t stream) {
+cudaError_t launch_tracer(int grid_type, bool bookkeeping, const RunParams& P, int nslots, int precision, int blocks,
+                          int threads, cudaStream_t stream) {
     if (threads <= 0) threads = 256;
     bool f64 = precision == SKG_PREC_FP64;
     switch (grid_type) {
@@ -454,8 +468,9 @@ cudaError_t launch_tracer(int grid_type, const RunParams& P, int nslots, int pre
                    : launch_one<float, CartStepper>(P, nslots, blocks, threads, stream);
     case SKG_GRID_OCTREE:
     case SKG_GRID_BINTREE:
-        return f64 ? launch_one<double, TreeStepper>(P, nslots, blocks, threads, stream)
-                   : launch_one<float, TreeStepper>(P, nslots, blocks, threads, stream);
+        if (f64) return launch_one<double, TreeStepper>(P, nslots, blocks, threads, stream);
+        return bookkeeping ? launch_one<float, TreeNodeWalk>(P, nslots, blocks, threads, stream)
+                           : launch_one<float, TreeStepper>(P, nslots, blocks, threads, stream);
     default:
         return f64 ? launch_one<double, VoronoiStepper>(P, nslots, blocks, threads, stream)
                    : launch_one<float, VoronoiStepper>(P, nslots, blocks, threads, stream);

@@ -87,8 +87,13 @@ def test_cartesian_fp32_against_fp64():
     tau32 = ctx.optical_depth(r, k, 0, A.PREC_FP32)
     ok = tau64 > 1e-3
     rel = np.abs(tau32[ok] - tau64[ok]) / tau64[ok]
-    # rays grazing a cell plane may credit a sliver of length to the neighbouring cell in FP32
-    assert np.mean(rel < 1e-5) > 0.999 and np.max(rel) < 1e-2, (np.mean(rel < 1e-5), np.max(rel))
+    # FP32 positions carry ~6e-8 of the 20 kpc half-width, i.e. ~1.5e-5 of an 80 pc z-cell, and a
+    # plane crossing of a ray at small |k_z| is uncertain by that over |k_z|: each crossing moves
+    # a sliver of path between two cells whose densities differ by tens of percent.  Stated error
+    # of the FP32 optical depth against FP64: below 1e-4 relative on 99.9% of the rays, below 1e-2
+    # on all of them, and the summed optical depth of all rays within 1e-6.
+    assert np.mean(rel < 1e-4) > 0.999 and np.max(rel) < 1e-2, (np.mean(rel < 1e-4), np.max(rel))
+    assert abs(tau32[ok].sum() / tau64[ok].sum() - 1) < 1e-6
     ctx.close()
 
 
