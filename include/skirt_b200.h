@@ -255,6 +255,26 @@ int  skg_read_density(skg_ctx* ctx, double* rho);
 int  skg_trace_paths(skg_ctx* ctx, const double* r, const double* k, int64_t n, int precision,
                      int32_t* cells, double* ds, int64_t* offsets, int64_t capacity);
 
+/* The same paths as skg_trace_paths for callers that cannot allocate device memory during a
+   call (a serving loop or host framework that owns a fixed HBM budget; cudaMalloc would
+   synchronise the device and can fail on a fragmented heap).  No counterpart in the reference:
+   it exists only because of how this library is embedded.
+   All pointers are DEVICE pointers: d_r[3n], d_k[3n] in; d_cells/d_ds (length capacity) and
+   d_offsets (n+1) out, with the same layout and values as skg_trace_paths.  The call allocates
+   nothing: its scratch (per-ray counts and scan totals, 8 MiB + 8 KiB) is a static device array
+   of this library, so n is limited to SKG_NOALLOC_MAX_RAYS (larger n returns SKG_ERR_CAPACITY
+   at once).  The device address of that array is looked up on the first call on each device;
+   make that first call before any stream capture.  The work is enqueued on `stream` (NULL =
+   the context's stream) and the call returns without waiting; once that stream has completed,
+   skg_sync(ctx, ...) reports SKG_ERR_CAPACITY when the segments exceed `capacity` (d_offsets[n]
+   then holds the needed total) or SKG_ERR_STEP_BUDGET.  All calls on one device share the one
+   scratch array: two calls whose work overlaps in time (different streams or threads, or
+   different contexts on the same device) race and corrupt each other's results. */
+#define SKG_NOALLOC_MAX_RAYS 1048576
+int  skg_trace_paths_noalloc(skg_ctx* ctx, const double* d_r, const double* d_k, int64_t n, int precision,
+                             int32_t* d_cells, double* d_ds, int64_t* d_offsets, int64_t capacity,
+                             void* stream);
+
 /* Optical depth from each r along k to the grid edge at wavelength ell (Instrument::opticalDepth ->
    DustSystem::opticaldepth, DustSystem.cpp:960-976). */
 int  skg_optical_depth(skg_ctx* ctx, const double* r, const double* k, int64_t n, int ell,

@@ -129,6 +129,8 @@ FUNCS = {
     "skg_ctx_info": (C.c_int, [C.c_void_p, i64p, i64p]),
     "skg_read_density": (C.c_int, [C.c_void_p, dp]),
     "skg_trace_paths": (C.c_int, [C.c_void_p, dp, dp, C.c_int64, C.c_int, i32p, dp, i64p, C.c_int64]),
+    "skg_trace_paths_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     "skg_optical_depth": (C.c_int, [C.c_void_p, dp, dp, C.c_int64, C.c_int, C.c_int, dp]),
     "skg_chunk_params": (C.c_int, [C.c_double, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint64),
                                    C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),

@@ -9,6 +9,8 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -1183,5 +1185,126 @@ int skg_batch_last_ms(skg_batch* b, float* ms) {
     return SKG_OK;
 }
 
+
+/* ---- path harness without device allocation ------------------------------------------------
+   skg_trace_paths allocates its staging and scan buffers on every call.  Callers that own all
+   of the device memory themselves -- a serving loop that reserves a fixed share of HBM up front,
+   or a host framework whose allocator must stay the only one, where a cudaMalloc in the middle
+   of a request would synchronise the device and could fail on a fragmented heap -- cannot use
+   it.  skg_trace_paths_noalloc takes device buffers from the caller and keeps its only scratch
+   (the per-ray segment counts, turned in place into offsets, and the scan's block totals) in the
+   file-scope array below, so the call performs no allocation at all.  The same count and write
+   kernels as skg_trace_paths produce the segments, hence the results are identical. */
+}  // extern "C"
+
+namespace {
+
+constexpr int NA_SCAN = 1024;                                         // rays per scan block
+constexpr int64_t NA_MAX_RAYS = SKG_NOALLOC_MAX_RAYS;
+constexpr int64_t NA_MAX_BLOCKS = NA_MAX_RAYS / NA_SCAN;
+static_assert(NA_MAX_RAYS % NA_SCAN == 0 && NA_MAX_BLOCKS <= NA_SCAN, "one block scans the block totals");
+
+// [0, NA_MAX_RAYS]: segment count of ray i, later the write offset of ray i (clamped to the
+// caller's capacity); [NA_MAX_RAYS + 1, +NA_MAX_BLOCKS): scan totals per block.  Every entry a
+// call reads is written earlier in that call, so nothing here has to start at zero.
+// 8 MiB + 8 KiB per device.
+static __device__ __align__(256) int64_t g_noalloc_scratch[NA_MAX_RAYS + 1 + NA_MAX_BLOCKS];
+
+std::mutex g_noalloc_mutex;
+int64_t* g_noalloc_addr[64] = {};
+
+__device__ int64_t na_block_inclusive_scan(int64_t v) {
+    __shared__ int64_t warp_tot[NA_SCAN / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+        int64_t u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) warp_tot[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        int64_t t = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            int64_t u = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += u;
+        }
+        warp_tot[lane] = t;
+    }
+    __syncthreads();
+    return v + (w > 0 ? warp_tot[w - 1] : 0);
+}
+
+// inclusive scan of the counts inside each block -> offsets[i + 1]; block totals -> scratch
+__global__ void na_scan_blocks(const int64_t* __restrict__ counts, int64_t n, int64_t* offsets, int64_t* block_tot) {
+    int64_t i = (int64_t)blockIdx.x * NA_SCAN + threadIdx.x;
+    int64_t v = na_block_inclusive_scan(i < n ? counts[i] : 0);
+    if (i < n) offsets[i + 1] = v;
+    if (threadIdx.x == NA_SCAN - 1) block_tot[blockIdx.x] = v;
+}
+
+// exclusive scan of the block totals (one block); flags a total above the capacity
+__global__ void na_scan_totals(int64_t* block_tot, int nblocks, int64_t capacity, unsigned* err) {
+    int64_t t = threadIdx.x < nblocks ? block_tot[threadIdx.x] : 0;
+    int64_t inc = na_block_inclusive_scan(t);
+    if (threadIdx.x < nblocks) block_tot[threadIdx.x] = inc - t;
+    if (threadIdx.x == nblocks - 1 && inc > capacity) atomicOr(err, ERR_CAPACITY);
+}
+
+// final offsets for the caller, and the same offsets clamped to the capacity for the write pass
+// (a ray whose segments do not fit then stops at the clamp and flags the overflow)
+__global__ void na_add_offsets(int64_t* offsets, const int64_t* __restrict__ block_pre, int64_t n,
+                               int64_t capacity, int64_t* woff) {
+    int64_t i = (int64_t)blockIdx.x * NA_SCAN + threadIdx.x;
+    if (i == 0) { offsets[0] = 0; woff[0] = 0; }
+    if (i >= n) return;
+    int64_t o = offsets[i + 1] + block_pre[blockIdx.x];
+    offsets[i + 1] = o;
+    woff[i + 1] = o < capacity ? o : capacity;
+}
+
+}  // namespace
+
+extern "C" {
+
+int skg_trace_paths_noalloc(skg_ctx* ctx, const double* d_r, const double* d_k, int64_t n, int precision,
+                            int32_t* d_cells, double* d_ds, int64_t* d_offsets, int64_t capacity, void* stream) {
+    if (n > NA_MAX_RAYS)
+        return fail(ctx, Failure{SKG_ERR_CAPACITY, "skg_trace_paths_noalloc: " + std::to_string(n) +
+                                 " rays exceed the per-call maximum of " + std::to_string(NA_MAX_RAYS)});
+    if (!ctx || n < 0 || capacity < 0 || !d_offsets || (n > 0 && (!d_r || !d_k)) || (capacity > 0 && (!d_cells || !d_ds)))
+        return fail(ctx, Failure{SKG_ERR_INVALID, "skg_trace_paths_noalloc: invalid arguments"});
+    try {
+        CK(cudaSetDevice(ctx->device));
+        REQUIRE(ctx->device >= 0 && ctx->device < 64, "device ordinal out of range");
+        int64_t* scratch;
+        {
+            // the scratch address of this device, looked up once (with the device current)
+            std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+            if (!g_noalloc_addr[ctx->device]) {
+                void* p = nullptr;
+                CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+                g_noalloc_addr[ctx->device] = (int64_t*)p;
+            }
+            scratch = g_noalloc_addr[ctx->device];
+        }
+        int64_t* block_tot = scratch + NA_MAX_RAYS + 1;
+        cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+        CK(cudaMemsetAsync(ctx->err, 0, sizeof(unsigned), s));
+        if (n == 0) {
+            CK(cudaMemsetAsync(d_offsets, 0, sizeof(int64_t), s));
+            return SKG_OK;
+        }
+        int nblocks = (int)((n + NA_SCAN - 1) / NA_SCAN);
+        CK(launch_count_segments(ctx->grid, d_r, d_k, n, precision, scratch, ctx->err, s));
+        na_scan_blocks<<<nblocks, NA_SCAN, 0, s>>>(scratch, n, d_offsets, block_tot);
+        CK(cudaGetLastError());
+        na_scan_totals<<<1, NA_SCAN, 0, s>>>(block_tot, nblocks, capacity, ctx->err);
+        CK(cudaGetLastError());
+        na_add_offsets<<<nblocks, NA_SCAN, 0, s>>>(d_offsets, block_tot, n, capacity, scratch);
+        CK(cudaGetLastError());
+        CK(launch_write_segments(ctx->grid, d_r, d_k, n, precision, scratch, d_cells, d_ds, ctx->err, s));
+        return SKG_OK;
+    } catch (const Failure& f) { return fail(ctx, f); }
+}
 
 }  // extern "C"

@@ -74,6 +74,16 @@ class Context:
         tot = int(off[n])
         return off, cells[:tot], ds[:tot]
 
+    NOALLOC_MAX_RAYS = 1048576
+
+    def trace_paths_noalloc(self, d_r, d_k, n, d_cells, d_ds, d_offsets, capacity, precision=A.PREC_FP64,
+                            stream=None):
+        """skg_trace_paths_noalloc: device addresses (ints) in and out; enqueues on `stream` (a
+        cudaStream_t as int, None = the context's stream) and returns without waiting.  The
+        status of the device work is reported by sync() after that stream has completed."""
+        self._ck(self.lib.skg_trace_paths_noalloc(self.h, d_r, d_k, n, precision, d_cells, d_ds, d_offsets,
+                                                  capacity, stream))
+
     def optical_depth(self, r, k, ell=0, precision=A.PREC_FP64):
         r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
         k = np.ascontiguousarray(k, dtype=np.float64).reshape(-1, 3)
