@@ -2,8 +2,8 @@
 disk galaxy (50 log-spaced wavelengths 0.1-10 micron, octree max level 10 with cell mass fraction
 < 1e-6, three 512x512 frames at 0/60/88 degrees, FP32 geometry with FP64 tallies).
 
-One step = one stellar-emission phase (one persistent launch) over all 50 wavelengths with
---packets packets per wavelength per GPU.  Ranks (torchrun, one per GPU) run disjoint packet
+One step = one stellar-emission phase (a sequence of waves: an event pass and a traversal pass
+each) over all 50 wavelengths with --packets packets per wavelength per GPU.  Ranks (torchrun, one per GPU) run disjoint packet
 ranges of one simulation and all-reduce the frames over NCCL at the end of each step (weak
 scaling: the packets per GPU are fixed).  `value` is device-timed; `e2e` is the same metric
 through the C ABI with the tallies read back into host memory every step.
@@ -269,19 +269,22 @@ def main():
     packets = Npp * nl * args.steps                # all ranks together
     value = packets / (total_ms / 1e3)
 
-    # per-launch kernel time and counters of the last step for the roofline
+    # kernel times and counters of one more step for the roofline: the traversal pass is the
+    # dominant kernel; its device time is summed over the waves of the phase (CUDA events around
+    # each launch on the launching stream)
     ctx.reset_tallies()
-    ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=999, precision=prec)
+    ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=999, precision=prec, stream=handle)
     ctx.sync()
     kms = ctx.last_phase_ms()
+    ev_ms, trav_ms, waves = ctx.phase_times()
     c = ctx.counters()
-    # algorithmic bytes (FP32 octree, neighbour search): per cell step the cell density (4 B) and the
-    # leaf box (24 B); per scanned neighbour entry its id (4 B) and box (24 B); per tally update 8 B
+    # algorithmic bytes of the traversal pass (FP32 octree): per cell step the leaf box (24 B) and
+    # the cell density (4 B) of the current leaf; per followed rope its id (4 B); per absorption
+    # tally 8 B (the FP64 walk reads 48 B boxes and 8 B densities)
     bstep = 4 + 24 if prec == A.PREC_FP32 else 8 + 48
-    bnbr = 4 + 24 if prec == A.PREC_FP32 else 4 + 48
-    alg_bytes = c["steps"] * bstep + c["nbr_scanned"] * bnbr + 8 * (c["absorb_adds"] + c["pixel_adds"])
+    alg_bytes = c["steps"] * bstep + c["nbr_scanned"] * 4 + 8 * c["absorb_adds"]
     peak, peak_kind = peaks()
-    achieved = alg_bytes / (kms / 1e3) / 1e9
+    achieved = alg_bytes / waves / (trav_ms / waves / 1e3) / 1e9 if waves else 0.0
 
     # ---- end to end through the C ABI with host buffers: reset, run, read the 3 frames to host
     cubes_bytes = sum(8 * nl * 512 * 512 for _ in range(3))
@@ -321,10 +324,13 @@ def main():
             "config": _config(args, tree),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": kms},
+                         "kernel": "trav_kernel (traversal pass)",
+                         "algorithmic_bytes_per_launch": alg_bytes / max(waves, 1),
+                         "kernel_ms_per_launch": trav_ms / max(waves, 1), "launches_per_step": waves,
+                         "phase_ms": kms, "event_pass_ms": ev_ms, "traversal_pass_ms": trav_ms},
             "e2e": {"value": e2e, "unit": "packets/s", "h2d_bytes_per_step": 4 * nl + 64,
                     "d2h_bytes_per_step": cubes_bytes},
-            "gpu_launches": args.steps,
+            "gpu_launches": 2 * waves * args.steps,
             "clocks": clk,
             "counters_last_step": c,
             "tree_build_s": tree_s,

@@ -208,10 +208,11 @@ typedef struct skg_run_opts {
     int32_t precision;                      /* SKG_PREC_* for the traversal geometry */
     int32_t max_steps;                      /* per traversal cell-step budget (0 = default 1<<20) */
     int32_t max_scatt;                      /* per packet scattering budget (0 = default 100000) */
-    int32_t blocks;                         /* 0 = auto (resident blocks x SM count) */
-    int32_t threads;                        /* 0 = auto (256) */
+    int32_t blocks;                         /* traversal blocks per wave (0 = auto: resident blocks x SMs) */
+    int32_t threads;                        /* reserved (0) */
     int32_t dedupe_peeloff;                 /* share one peel-off traversal among instruments that see
                                                the packet from the same direction (same tau; default 1) */
+    int32_t pool;                           /* packets in flight per wave (0 = default 2^21) */
 } skg_run_opts;
 
 /* Counters of one phase run (device side, exact). */
@@ -226,6 +227,7 @@ typedef struct skg_counters {
     uint64_t nbr_scanned;                   /* neighbour-list entries scanned (tree/Voronoi) */
     uint64_t fallbacks;                     /* neighbour search fallbacks / re-locations */
     uint64_t errors;                        /* packets retired on a budget or NaN */
+    uint64_t waves;                         /* waves (event pass + traversal pass) of the phase */
 } skg_counters;
 
 typedef struct skg_ctx skg_ctx;
@@ -345,6 +347,10 @@ int  skg_read_counters(skg_ctx* ctx, skg_counters* out);
 int  skg_sync(skg_ctx* ctx, int timeout_ms);
 /* Device time (ms) of the last skg_run_phase launch (CUDA events on the launching stream). */
 int  skg_last_phase_ms(skg_ctx* ctx, float* ms);
+/* The last phase split by kernel: summed device time (ms) of its event passes (launch, detection,
+   scattering) and of its traversal passes, and its number of waves (each wave is one launch of
+   each).  Finishes the phase first. */
+int  skg_phase_times(skg_ctx* ctx, float* event_ms, float* traversal_ms, int32_t* waves);
 
 /* ---- dust emission (PanDustSystem::calculatedustemission / DustLib::calculate) --------- */
 /* From the absorbed luminosity held in the context computes, per cell, the mean intensity

@@ -102,14 +102,14 @@ class Scene(C.Structure):
 class RunOpts(C.Structure):
     _fields_ = [
         ("precision", C.c_int32), ("max_steps", C.c_int32), ("max_scatt", C.c_int32),
-        ("blocks", C.c_int32), ("threads", C.c_int32), ("dedupe_peeloff", C.c_int32),
+        ("blocks", C.c_int32), ("threads", C.c_int32), ("dedupe_peeloff", C.c_int32), ("pool", C.c_int32),
     ]
 
 
 class Counters(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "packets", "steps", "traversals", "scatterings", "peeloffs", "absorb_adds", "pixel_adds",
-        "nbr_scanned", "fallbacks", "errors")]
+        "nbr_scanned", "fallbacks", "errors", "waves")]
 
 
 class Work(C.Structure):
@@ -151,6 +151,7 @@ FUNCS = {
     "skg_read_counters": (C.c_int, [C.c_void_p, C.POINTER(Counters)]),
     "skg_sync": (C.c_int, [C.c_void_p, C.c_int]),
     "skg_last_phase_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "skg_phase_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), i32p]),
     "skg_calc_dust_emission": (C.c_int, [C.c_void_p, dp]),
     "skg_absorbed_totals": (C.c_int, [C.c_void_p, dp, dp]),
     "skg_reset_dust_absorption": (C.c_int, [C.c_void_p]),

@@ -3,6 +3,7 @@
 #include "skg_scene.cuh"
 #include "skg_internal.h"
 #include "skg_tree.h"
+#include "skg_wave.h"
 
 #include <algorithm>
 #include <chrono>
@@ -310,6 +311,8 @@ struct skg_ctx {
     unsigned long long* counters = nullptr;   // = own.counters
     unsigned* err = nullptr;                  // = own.err
     Staging own;                              // tables of this context's own launches
+    WaveRunner waves;                         // packet pool and job lists of this context's phases
+    uint64_t wave_count = 0;                  // waves since the last tally reset
     std::vector<double> lambda, dlambda;
     // dust emission
     int nT = 0;
@@ -323,6 +326,19 @@ static int fail(skg_ctx* ctx, const Failure& f) {
     set_error(f.msg);
     if (ctx) ctx->error = f.msg;
     return f.code;
+}
+
+// Completes the context's running phase: waits for its enqueued waves and adds waves until no
+// packet is left (the reads, resets and the next phase need the finished tallies).
+static int settle(skg_ctx* ctx, int timeout_ms) {
+    if (!ctx->waves.pending()) return SKG_OK;
+    cudaSetDevice(ctx->device);
+    bool timed_out = false;
+    cudaError_t e = ctx->waves.finish(timeout_ms, ctx->ev1, &timed_out);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, Failure{SKG_ERR_CUDA, cudaGetErrorString(e)}); }
+    if (timed_out) return fail(ctx, Failure{SKG_ERR_TIMEOUT, "timed out waiting for the device"});
+    ctx->wave_count += ctx->waves.waves();
+    return SKG_OK;
 }
 
 extern "C" {
@@ -360,6 +376,7 @@ int skg_ctx_create(const skg_scene* sc, int device, skg_ctx** out) {
         CK(cudaSetDevice(device));
         CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
         CK(cudaEventCreate(&ctx->ev0)); CK(cudaEventCreate(&ctx->ev1));
+        ctx->waves.timing = true;
         cudaStream_t s = ctx->stream;
         Allocs& A = ctx->A;
 
@@ -596,6 +613,8 @@ int skg_ctx_info(const skg_ctx* ctx, int64_t* ncells, int64_t* device_bytes) {
 
 int skg_sync(skg_ctx* ctx, int timeout_ms) {
     if (!ctx) return SKG_ERR_INVALID;
+    int rc = settle(ctx, timeout_ms);
+    if (rc) return rc;
     cudaSetDevice(ctx->device);
     auto t0 = std::chrono::steady_clock::now();
     while (true) {
@@ -683,6 +702,8 @@ int skg_optical_depth(skg_ctx* ctx, const double* r, const double* k, int64_t n,
 int skg_run_phase(skg_ctx* ctx, int phase, const int32_t* ells, int nell, uint64_t npp, uint64_t first_packet,
                   uint64_t count, uint64_t seed, const skg_run_opts* opts, void* stream) {
     if (!ctx) return SKG_ERR_INVALID;
+    int rc = settle(ctx, -1);
+    if (rc) return rc;
     try {
         CK(cudaSetDevice(ctx->device));
         REQUIRE(phase >= SKG_PHASE_STELLAR && phase <= SKG_PHASE_DUST_EMISSION, "unknown phase");
@@ -690,10 +711,15 @@ int skg_run_phase(skg_ctx* ctx, int phase, const int32_t* ells, int nell, uint64
         for (int i = 0; i < nell; i++) REQUIRE(ells[i] >= 0 && ells[i] < ctx->nlambda, "wavelength index out of range");
         REQUIRE(count <= npp || npp == 0, "packet range exceeds the packet count");
         if (phase != SKG_PHASE_STELLAR) REQUIRE(ctx->emit_cdf != nullptr, "dust phases need dust emission enabled");
+        REQUIRE(!opts || opts->pool >= 0, "negative packet pool");
         cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
         if (count == 0) return SKG_OK;
+        const uint64_t total = (uint64_t)nell * count;
+        const size_t pool_max = (opts && opts->pool > 0) ? (size_t)opts->pool : ((size_t)1 << 21);
+        const size_t npool = (size_t)std::min<uint64_t>(total, pool_max);
+        CK(ctx->waves.reserve(npool, ctx->hs.ngroups));
         // one slot, one work item (pageable host sources: the copies are staged before return)
-        BatchHeader H = {phase, 1, 1, 0, (uint64_t)nell * count};
+        BatchHeader H = {phase, 1, 1, 0, total};
         WorkItem W;
         std::memset(&W, 0, sizeof(W));
         W.slot = 0; W.nell = nell; W.ell0 = 0; W.npp_total = npp; W.first = first_packet; W.count = count;
@@ -711,9 +737,9 @@ int skg_run_phase(skg_ctx* ctx, int phase, const int32_t* ells, int nell, uint64
         CK(cudaMemsetAsync(T.err, 0, sizeof(unsigned), s));
         RunParams P = T.params((opts && opts->max_scatt > 0) ? opts->max_scatt : 100000);
         int precision = opts ? opts->precision : SKG_PREC_FP32;
-        int blocks = opts ? opts->blocks : 0, threads = opts ? opts->threads : 0;
+        int blocks = opts ? opts->blocks : 0;
         CK(cudaEventRecord(ctx->ev0, s));
-        CK(launch_tracer(ctx->grid.type, ctx->grid.search == SKG_SEARCH_BOOKKEEPING, P, 1, precision, blocks, threads, s));
+        CK(ctx->waves.begin(P, ctx->grid.type, ctx->grid.search == SKG_SEARCH_BOOKKEEPING, precision, 1, npool, blocks, s));
         CK(cudaEventRecord(ctx->ev1, s));
         return SKG_OK;
     } catch (const Failure& f) { return fail(ctx, f); }
@@ -721,6 +747,8 @@ int skg_run_phase(skg_ctx* ctx, int phase, const int32_t* ells, int nell, uint64
 
 int skg_last_phase_ms(skg_ctx* ctx, float* ms) {
     if (!ctx || !ms) return SKG_ERR_INVALID;
+    int rc = settle(ctx, -1);
+    if (rc) return rc;
     cudaSetDevice(ctx->device);
     cudaError_t e = cudaEventSynchronize(ctx->ev1);
     if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, Failure{SKG_ERR_CUDA, cudaGetErrorString(e)}); }
@@ -728,8 +756,22 @@ int skg_last_phase_ms(skg_ctx* ctx, float* ms) {
     return SKG_OK;
 }
 
+int skg_phase_times(skg_ctx* ctx, float* event_ms, float* traversal_ms, int32_t* waves) {
+    if (!ctx) return SKG_ERR_INVALID;
+    int rc = settle(ctx, -1);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = ctx->waves.times(event_ms, traversal_ms);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, Failure{SKG_ERR_CUDA, cudaGetErrorString(e)}); }
+    if (waves) *waves = ctx->waves.waves();
+    return SKG_OK;
+}
+
 int skg_reset_tallies(skg_ctx* ctx) {
     if (!ctx) return SKG_ERR_INVALID;
+    int rc = settle(ctx, -1);
+    if (rc) return rc;
+    ctx->wave_count = 0;
     try {
         CK(cudaSetDevice(ctx->device));
         cudaStream_t s = ctx->stream;
@@ -766,6 +808,8 @@ int skg_read_instrument(skg_ctx* ctx, int instr, double* cube, double* sed) {
 
 int skg_read_instrument_device(skg_ctx* ctx, int instr, double* d_cube, double* d_sed, void* stream) {
     if (!ctx || instr < 0 || instr >= ctx->hs.ninstr) return SKG_ERR_INVALID;
+    int rc = settle(ctx, -1);
+    if (rc) return rc;
     try {
         CK(cudaSetDevice(ctx->device));
         cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
@@ -804,11 +848,14 @@ int skg_read_counters(skg_ctx* ctx, skg_counters* out) {
     cudaMemcpy(c, ctx->counters, sizeof(c), cudaMemcpyDeviceToHost);
     out->packets = c[0]; out->steps = c[1]; out->traversals = c[2]; out->scatterings = c[3]; out->peeloffs = c[4];
     out->absorb_adds = c[5]; out->pixel_adds = c[6]; out->nbr_scanned = c[7]; out->fallbacks = c[8]; out->errors = c[9];
+    out->waves = ctx->wave_count;
     return rc;
 }
 
 int skg_calc_dust_emission(skg_ctx* ctx, double* temperature) {
     if (!ctx) return SKG_ERR_INVALID;
+    int rc = settle(ctx, -1);
+    if (rc) return rc;
     try {
         CK(cudaSetDevice(ctx->device));
         REQUIRE(ctx->emit_cdf != nullptr, "dust emission is not enabled for this scene");
@@ -825,6 +872,8 @@ int skg_calc_dust_emission(skg_ctx* ctx, double* temperature) {
 
 int skg_absorbed_totals(skg_ctx* ctx, double* tot_stel, double* tot_dust) {
     if (!ctx) return SKG_ERR_INVALID;
+    int rc = settle(ctx, -1);
+    if (rc) return rc;
     try {
         CK(cudaSetDevice(ctx->device));
         cudaStream_t s = ctx->stream;
@@ -844,6 +893,8 @@ int skg_absorbed_totals(skg_ctx* ctx, double* tot_stel, double* tot_dust) {
 
 int skg_reset_dust_absorption(skg_ctx* ctx) {
     if (!ctx) return SKG_ERR_INVALID;
+    int rc = settle(ctx, -1);
+    if (rc) return rc;
     try {
         CK(cudaSetDevice(ctx->device));
         if (ctx->hs.labs_dust)
@@ -983,8 +1034,13 @@ struct skg_batch {
     int* h_ells = nullptr;
     cudaEvent_t copied = nullptr;          // the previous launch's tables have been read
     cudaGraphExec_t graph = nullptr;
-    int g_type = -1, g_bk = -1, g_prec = -1, g_blocks = -1, g_threads = -1;
+    int g_type = -1, g_bk = -1, g_prec = -1, g_blocks = -1;
+    size_t g_npool = 0;
+    int g_waves = 0;                       // waves captured in the graph
+    bool g_stale = false;                  // a replay needed more waves than captured
     cudaStream_t g_stream = nullptr;
+    WaveRunner waves;
+    uint64_t wave_count = 0;
     std::string error;
 };
 
@@ -992,6 +1048,19 @@ static int bfail(skg_batch* b, const Failure& f) {
     set_error(f.msg);
     if (b) b->error = f.msg;
     return f.code;
+}
+
+// Completes the batch's running phase (see settle for contexts).
+static int bsettle(skg_batch* b, int timeout_ms) {
+    if (!b->waves.pending()) return SKG_OK;
+    cudaSetDevice(b->device);
+    bool timed_out = false;
+    cudaError_t e = b->waves.finish(timeout_ms, b->ev1, &timed_out);
+    if (e != cudaSuccess) { cudaGetLastError(); return bfail(b, Failure{SKG_ERR_CUDA, cudaGetErrorString(e)}); }
+    if (timed_out) return bfail(b, Failure{SKG_ERR_TIMEOUT, "timed out waiting for the device"});
+    b->wave_count = b->waves.waves();
+    if (b->graph && b->waves.waves() > b->g_waves) b->g_stale = true;
+    return SKG_OK;
 }
 
 extern "C" {
@@ -1052,6 +1121,8 @@ int skg_batch_destroy(skg_batch* b) {
 int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, const skg_run_opts* opts, int flags,
                   void* stream) {
     if (!b) return SKG_ERR_INVALID;
+    int rc = bsettle(b, -1);
+    if (rc) return rc;
     try {
         CK(cudaSetDevice(b->device));
         REQUIRE(phase >= SKG_PHASE_STELLAR && phase <= SKG_PHASE_DUST_EMISSION, "unknown phase");
@@ -1100,13 +1171,18 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
         }
         *b->h_hdr = BatchHeader{phase, nslots, nwork, 0, total};
         int precision = opts ? opts->precision : SKG_PREC_FP32;
-        int blocks = opts ? opts->blocks : 0, threads = opts ? opts->threads : 0;
-        if (blocks <= 0) {
-            int sms = 0;
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-            blocks = sms * 3;       // three 256-thread blocks per SM (the tracer's launch bounds)
-        }
-        if (threads <= 0) threads = 256;
+        int blocks = opts ? opts->blocks : 0;
+        REQUIRE(!opts || opts->pool >= 0, "negative packet pool");
+        // the pool: enough records for the batch up to the pool limit, rounded up to a power of two
+        // so that replays of a captured graph keep fitting
+        const size_t pool_max = (opts && opts->pool > 0) ? (size_t)opts->pool : ((size_t)1 << 21);
+        size_t npool = 1;
+        while (npool < total && npool < pool_max) npool <<= 1;
+        npool = std::min(npool, pool_max);
+        int ngroups = 0;
+        for (skg_ctx* c : slots) ngroups = std::max(ngroups, c->hs.ngroups);
+        if (total == 0) return SKG_OK;
+        CK(b->waves.reserve(npool, ngroups));
         RunParams P = b->T.params((opts && opts->max_scatt > 0) ? opts->max_scatt : 100000);
         Staging& T = b->T;
         auto enqueue = [&](cudaStream_t q) {
@@ -1118,13 +1194,13 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
             CK(cudaMemsetAsync(T.work, 0, sizeof(unsigned long long), q));
             CK(cudaMemsetAsync(T.err, 0, sizeof(unsigned), q));
             // every slot's DevGrid is copied into shared memory: size for the batch's capacity
-            CK(launch_tracer(gtype < 0 ? SKG_GRID_CARTESIAN : gtype, gbk == 1, P, T.max_slots, precision, blocks,
-                             threads, q));
+            CK(b->waves.begin(P, gtype < 0 ? SKG_GRID_CARTESIAN : gtype, gbk == 1, precision, T.max_slots, npool,
+                              blocks, q));
         };
         CK(cudaEventRecord(b->ev0, s));
         if (flags & SKG_BATCH_GRAPH) {
-            bool same = b->graph && b->g_type == gtype && b->g_bk == gbk && b->g_prec == precision && b->g_blocks == blocks &&
-                        b->g_threads == threads;
+            bool same = b->graph && !b->g_stale && b->g_type == gtype && b->g_bk == gbk && b->g_prec == precision &&
+                        b->g_blocks == blocks && b->g_npool == npool;
             if (!same) {
                 if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
                 if (!b->g_stream) CK(cudaStreamCreateWithFlags(&b->g_stream, cudaStreamNonBlocking));
@@ -1135,9 +1211,11 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
                 cudaError_t e = cudaGraphInstantiate(&b->graph, gr, 0);
                 cudaGraphDestroy(gr);
                 CK(e);
-                b->g_type = gtype; b->g_bk = gbk; b->g_prec = precision; b->g_blocks = blocks; b->g_threads = threads;
+                b->g_type = gtype; b->g_bk = gbk; b->g_prec = precision; b->g_blocks = blocks; b->g_npool = npool;
+                b->g_waves = b->waves.waves(); b->g_stale = false;
             }
             CK(cudaGraphLaunch(b->graph, s));
+            b->waves.replayed(s, b->g_waves);       // the replay runs the captured waves on s
         } else {
             enqueue(s);
         }
@@ -1149,6 +1227,8 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
 
 int skg_batch_sync(skg_batch* b, int timeout_ms) {
     if (!b) return SKG_ERR_INVALID;
+    int rc = bsettle(b, timeout_ms);
+    if (rc) return rc;
     cudaSetDevice(b->device);
     auto t0 = std::chrono::steady_clock::now();
     while (true) {
@@ -1173,11 +1253,14 @@ int skg_batch_counters(skg_batch* b, skg_counters* out) {
     cudaMemcpy(c, b->T.counters, sizeof(c), cudaMemcpyDeviceToHost);
     out->packets = c[0]; out->steps = c[1]; out->traversals = c[2]; out->scatterings = c[3]; out->peeloffs = c[4];
     out->absorb_adds = c[5]; out->pixel_adds = c[6]; out->nbr_scanned = c[7]; out->fallbacks = c[8]; out->errors = c[9];
+    out->waves = b->wave_count;
     return rc;
 }
 
 int skg_batch_last_ms(skg_batch* b, float* ms) {
     if (!b || !ms) return SKG_ERR_INVALID;
+    int rc = bsettle(b, -1);
+    if (rc) return rc;
     cudaSetDevice(b->device);
     cudaError_t e = cudaEventSynchronize(b->ev1);
     if (e != cudaSuccess) { cudaGetLastError(); return bfail(b, Failure{SKG_ERR_CUDA, cudaGetErrorString(e)}); }

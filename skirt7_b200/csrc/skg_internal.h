@@ -12,11 +12,6 @@ struct DevGrid;
 struct DevScene;
 struct RunParams;
 
-// skg_tracer.cu
-// bookkeeping: the slots' trees use the Bookkeeping search (the FP32 launch then walks nodes)
-cudaError_t launch_tracer(int grid_type, bool bookkeeping, const RunParams& P, int nslots, int precision, int blocks,
-                          int threads, cudaStream_t stream);
-
 // skg_trace.cu (compiled with --fmad=false: bit-exact FP64 traversal)
 cudaError_t launch_count_segments(const DevGrid& g, const double* r, const double* k, int64_t n,
                                   int precision, int64_t* counts, unsigned* err, cudaStream_t s);

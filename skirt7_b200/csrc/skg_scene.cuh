@@ -115,6 +115,49 @@ struct RunParams {
 };
 
 // ---------------------------------------------------------------------------------------------
+// Wavefront state.  The packets in flight live in a pool of 128-byte records; each wave an event
+// pass (one thread per record) advances every packet to its next traversals and writes them as
+// jobs, and a traversal pass walks all jobs of the wave.
+enum PacketState : int { PK_EMPTY = 0, PK_WAIT, PK_INTERACT, PK_TERM, PK_DONE };
+constexpr int JOB_MAIN = 31;          // job type of the packet's own path; 0..15 = peel-off group
+
+struct __align__(16) Packet {
+    double x, y, z;                   // position (rounded to the traversal precision)
+    double kx, ky, kz;                // direction
+    double L, Lth;                    // luminosity and its termination threshold
+    double s_int;                     // distance to the interaction point (result of the path job)
+    uint64_t id;                      // packet number within its work item (RNG counter words)
+    int item;                         // work item
+    int ell;
+    int nscatt;
+    int pos_cell;                     // cell of the position: -2 unknown, -1 outside the grid
+    int int_cell;                     // cell of the interaction point (-1 unknown)
+    unsigned rngc;                    // next Philox block of the packet's stream
+    int state;                        // PacketState
+    int flags;                        // bit 0 stellar origin, bit 1 the pending peel-offs follow a scattering
+    int peel_j0, peel_n;              // this packet's peel-off jobs of the last wave
+    int pad[2];
+};
+static_assert(sizeof(Packet) == 128, "packet record is two 64-byte lines");
+
+struct WaveParams {
+    RunParams R;
+    Packet* pk;
+    int npool;
+    int wave;                         // index of this wave within the phase
+    // this wave's jobs (written by the event pass, walked by the traversal pass)
+    int2* jobs;                       // (packet, type)
+    double* jtau;                     // peel-off optical depth
+    double* jL;                       // peel-off luminosity
+    unsigned* jcount;                 // [0] jobs, [1] jobs taken by the traversal pass, [2] packets with jobs
+    // the previous wave's jobs (peel-off detection)
+    const int2* pjobs;
+    const double* pjtau;
+    const double* pjL;
+    unsigned* last_busy;              // highest wave index that had jobs
+};
+
+// ---------------------------------------------------------------------------------------------
 // samplers
 
 // Lambert W, branch -1, on [-1/e, 0) (the function SpecialFunctions::LambertW1 evaluates,

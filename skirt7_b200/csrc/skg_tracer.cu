@@ -1,39 +1,46 @@
-// skg_tracer.cu -- the persistent photon-packet tracer.
+// skg_tracer.cu -- the wavefront photon-packet tracer.
 //
-// One launch runs a whole phase (stellar emission, dust self-absorption or dust emission) for a
-// batch of wavelengths of one or more simulations: it replaces
-// Parallel::call(this, &dostellaremissionchunk, Nlambda, Nchunks) (MonteCarloSimulation.cpp:241-295)
-// and the two dust chunk bodies (PanMonteCarloSimulation.cpp:191-346).  Each thread carries one
-// packet at a time through an explicit state machine:
+// One phase (stellar emission, dust self-absorption or dust emission) of a batch of wavelengths of
+// one or more simulations replaces Parallel::call(this, &dostellaremissionchunk, Nlambda, Nchunks)
+// (MonteCarloSimulation.cpp:241-295) and the two dust chunk bodies
+// (PanMonteCarloSimulation.cpp:191-346).  The life cycle of a packet,
 //
-//   FETCH -> launch -> PEEL(emission) x groups -> MAIN1 -> [terminate?] -> MAIN2 -> PEEL(scattering)
-//         -> SCATTER -> MAIN1 -> ...
+//   launch -> peel-off (emission) -> path: absorption, escape fraction, termination test, forced
+//   interaction point -> propagate -> peel-off (scattering) -> scatter -> path -> ...
 //
-// and every lane of a warp executes the same cell-step code whatever traversal it is on (a
-// peel-off ray, the full path of the packet, or the re-walk to the interaction point), so the
-// inner loop stays converged.  Cell steps never materialise the segment list:
-//   MAIN1 streams kappa*rho*ds into the FP64 cumulative optical depth and the per-cell absorption
-//         tallies (MonteCarloSimulation::simulateescapeandabsorption, :432-509);
-//   MAIN2 re-walks the same path until the cumulative optical depth passes the sampled one and
-//         interpolates inside that segment -- DustGridPath::pathlength (DustGridPath.cpp:162-173);
-//   PEEL  accumulates the optical depth towards an observer (DustSystem::opticaldepth, :960-976).
-// Instruments seen from the same direction share one peel-off traversal (identical optical
-// depth; the reference recomputes it per instrument).  The event code (launch samplers,
-// scattering, detection) sits in non-inlined functions so that the step loop keeps few registers.
+// is cut at its traversals.  The packets in flight sit in a pool of 128-byte records.  Each wave
+// runs two kernels:
+//   event_kernel  one thread per record: detects the peel-offs walked in the previous wave, moves
+//                 a scattered packet to its interaction point, writes the scattering peel-offs,
+//                 scatters, or launches a new packet into a free record; then appends the packet's
+//                 next traversals to the wave's job list (one peel-off job per direction group and
+//                 one path job);
+//   trav_kernel   persistent; each lane takes jobs one after another and walks them:
+//                 peel-off  accumulates the optical depth towards an observer
+//                           (DustSystem::opticaldepth, DustSystem.cpp:960-976);
+//                 path      streams kappa*rho*ds into the FP64 cumulative optical depth and the
+//                           per-cell absorption tallies (simulateescapeandabsorption, :432-509),
+//                           applies the escape fraction and the termination test, samples the
+//                           interaction optical depth (simulatepropagation, :513-531) and re-walks
+//                           the path to the segment where the cumulative optical depth passes it,
+//                           interpolating inside it (DustGridPath::pathlength, DustGridPath.cpp:162-173).
+// The traversal kernel holds nothing but the walk, so it keeps few registers, no local memory and
+// a small instruction footprint; the divergent event code runs once per packet per wave in a
+// kernel of its own.  Instruments seen from the same direction share one peel-off traversal
+// (identical optical depth; the reference recomputes it per instrument).
 #include "skg_scene.cuh"
 #include "skg_internal.h"
+#include "skg_wave.h"
+
+#include <chrono>
+#include <thread>
 
 namespace skg {
 
-#ifndef SKG_EVENT_LANES
-#define SKG_EVENT_LANES 32
-#endif
-#ifndef SKG_TRACER_MIN_BLOCKS
-#define SKG_TRACER_MIN_BLOCKS 3
+#ifndef SKG_TRAV_MIN_BLOCKS
+#define SKG_TRAV_MIN_BLOCKS 3
 #endif
 
-enum Mode : int { M_FETCH = 0, M_LAUNCH, M_PEEL_NEXT, M_MAIN1_START, M_AFTER_MAIN1, M_AFTER_MAIN2, M_SCATTER, M_DONE };
-enum Trav : int { T_NONE = 0, T_PEEL, T_MAIN1, T_MAIN2 };
 enum Cnt : int { C_PACKETS = 0, C_STEPS, C_TRAV, C_SCATT, C_PEEL, C_ABS, C_PIX, C_NBR, C_FB, C_ERR, C_N };
 
 template<typename R> SKG_D double rho_load(const DevScene& S, size_t i);
@@ -223,165 +230,277 @@ SKG_D int find_item(const WorkItem* items, int n, uint64_t p) {
     return lo;
 }
 
+// ---------------------------------------------------------------------------------------------
+// event pass
+
+// The direction groups that get a peel-off traversal from (x, y, z), in group order
+// (MonteCarloSimulation.cpp:299-357): emission peel-offs carry weight 1, scattering peel-offs the
+// phase-function value, and a negative value ends the list (the reference aborts the peel-off).
+// With WRITE the jobs are stored from j0 on; returns their number.
+template<bool WRITE>
+SKG_D int peel_jobs(const DevScene& S, int ell, bool scat, int cell, double kx, double ky, double kz, double x,
+                    double y, double z, double L, int p, int j0, int2* jobs, double* jL) {
+    int n = 0;
+    for (int g = 0; g < S.ngroups; g++) {
+        double w = 1.0;
+        if (scat) {
+            w = peel_weight(S, ell, cell, kx, ky, kz, S.gkx[g], S.gky[g], S.gkz[g]);
+            if (w < 0) break;
+        }
+        if (!group_needs_traversal(S, g, x, y, z)) continue;
+        if (WRITE) { jobs[j0 + n] = make_int2(p, g); jL[j0 + n] = L * w; }
+        n++;
+    }
+    return n;
+}
+
+template<typename R>
+__global__ void __launch_bounds__(256) event_kernel(const WaveParams W) {
+    __shared__ unsigned long long s_cnt[C_N];
+    if (threadIdx.x < C_N) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const RunParams& P = W.R;
+    const BatchHeader H = *P.hdr;
+    const int phase = H.phase;
+    const bool peel_on = phase != SKG_PHASE_DUST_SELFABS;
+    const int lane = threadIdx.x & 31;
+    const unsigned FULL = 0xffffffffu;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+
+    Packet K;
+    int state = PK_DONE;
+    if (p < W.npool) { K = W.pk[p]; state = K.state; }
+    const bool was_live = state != PK_DONE;
+    if (state == PK_WAIT) {                       // a path job that was not walked: drop the packet
+        atomicOr(P.err, ERR_CAPACITY); atomicAdd(&s_cnt[C_ERR], 1ull); state = PK_TERM;
+    }
+
+    // 1. the peel-offs walked in the previous wave (Instrument::detect of every group member)
+    if (was_live && K.peel_n > 0) {
+        const DevScene& S = *P.scenes[P.items[K.item].slot];
+        const int nsp = (K.flags & 2) ? K.nscatt : 0;   // the peel-off copy counts the scattering
+        int pix = 0;
+        for (int i = 0; i < K.peel_n; i++) {
+            const int j = K.peel_j0 + i;
+            pix += detect_group(S, W.pjobs[j].y, K.ell, W.pjL[j], W.pjtau[j], nsp, (K.flags & 1) != 0, K.x, K.y, K.z);
+        }
+        atomicAdd(&s_cnt[C_PIX], (unsigned long long)pix);
+        atomicAdd(&s_cnt[C_PEEL], (unsigned long long)K.peel_n);
+        K.peel_n = 0;
+    }
+
+    // 2. a packet at its interaction point: propagate, count its scattering peel-offs, scatter
+    int npeel = 0, nmain = 0;
+    bool scat_peel = false;
+    double kx0 = 0, ky0 = 0, kz0 = 0;              // direction before the scattering
+    if (state == PK_INTERACT) {
+        const WorkItem& It = P.items[K.item];
+        const DevScene& S = *P.scenes[It.slot];
+        const R si = (R)K.s_int;                    // PhotonPackage::propagate
+        K.x = (double)((R)K.x + si * (R)K.kx);
+        K.y = (double)((R)K.y + si * (R)K.ky);
+        K.z = (double)((R)K.z + si * (R)K.kz);
+        // the interaction point lies in the cell of its segment (verified by the stepper)
+        if (K.s_int > 0) K.pos_cell = (K.int_cell >= 0) ? K.int_cell : -2;
+        kx0 = K.kx; ky0 = K.ky; kz0 = K.kz;
+        if (peel_on) {
+            scat_peel = true;
+            npeel = peel_jobs<false>(S, K.ell, true, K.int_cell, kx0, ky0, kz0, K.x, K.y, K.z, K.L, 0, 0, nullptr,
+                                     nullptr);
+        }
+        Philox rng;
+        rng.init(It.seed, K.id, (uint32_t)K.ell | ((uint32_t)phase << 24));
+        rng.c0 = K.rngc;
+        const V3<double> kn = scatter_direction(S, K.ell, K.int_cell, mk3(K.kx, K.ky, K.kz), rng);
+        K.rngc = rng.c0;
+        K.kx = (double)(R)kn.x; K.ky = (double)(R)kn.y; K.kz = (double)(R)kn.z;
+        K.nscatt++;
+        atomicAdd(&s_cnt[C_SCATT], 1ull);
+        nmain = 1;
+        state = PK_WAIT;
+    }
+
+    // 3. free records take new packets: one work-counter atomic per warp; a launch with zero
+    //    luminosity takes the next packet
+    bool need = state == PK_EMPTY || state == PK_TERM;
+    while (__any_sync(FULL, need)) {
+        const unsigned want = __ballot_sync(FULL, need);
+        const int leader = __ffs(want) - 1;
+        unsigned long long base = 0;
+        if (lane == leader) base = atomicAdd(P.work, (unsigned long long)__popc(want));
+        base = __shfl_sync(FULL, base, leader);
+        if (need) {
+            const uint64_t gp = base + __popc(want & ((1u << lane) - 1));
+            if (gp >= H.total) {
+                state = PK_DONE; need = false;
+            } else {
+                const int it = find_item(P.items, H.nitems, gp);
+                const WorkItem It = P.items[it];
+                const uint64_t q = gp - It.begin;
+                const int ei = (int)(q / It.count);
+                const uint64_t ip = It.first + (q - (uint64_t)ei * It.count);
+                const int ell = P.ells[It.ell0 + ei];
+                Philox rng;
+                rng.init(It.seed, ip, (uint32_t)ell | ((uint32_t)phase << 24));
+                atomicAdd(&s_cnt[C_PACKETS], 1ull);
+                const DevScene& S = *P.scenes[It.slot];
+                const Launched o = launch_packet(P.grids[It.slot], S, phase, ell, It.npp_total, rng);
+                if (o.ok) {
+                    K.x = (double)(R)o.x; K.y = (double)(R)o.y; K.z = (double)(R)o.z;
+                    K.kx = (double)(R)o.kx; K.ky = (double)(R)o.ky; K.kz = (double)(R)o.kz;
+                    K.L = o.L; K.Lth = o.Lth; K.s_int = 0;
+                    K.id = ip; K.item = it; K.ell = ell; K.nscatt = 0;
+                    K.pos_cell = -2; K.int_cell = -1; K.rngc = rng.c0;
+                    K.flags = o.stellar ? 1 : 0; K.peel_n = 0;
+                    npeel = peel_on ? peel_jobs<false>(S, ell, false, -1, 0, 0, 0, K.x, K.y, K.z, K.L, 0, 0, nullptr,
+                                                       nullptr)
+                                    : 0;
+                    nmain = S.ncomp > 0 ? 1 : 0;            // without dust the life cycle ends here
+                    state = nmain ? PK_WAIT : PK_TERM;
+                    need = false;
+                }
+            }
+        }
+    }
+
+    // 4. append the jobs: one reservation per warp, each packet's jobs contiguous
+    const int n = npeel + nmain;
+    int incl = n;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int tot = __shfl_sync(FULL, incl, 31);
+    unsigned base = 0;
+    if (lane == 31 && tot > 0) base = atomicAdd(W.jcount, (unsigned)tot);
+    base = __shfl_sync(FULL, base, 31);
+    const unsigned busy = __ballot_sync(FULL, n > 0);
+    if (lane == 0 && busy) {
+        atomicAdd(W.jcount + 2, (unsigned)__popc(busy));
+        atomicMax(W.last_busy, (unsigned)W.wave);
+    }
+    if (n > 0) {
+        const int j0 = (int)(base + incl - n);
+        const DevScene& S = *P.scenes[P.items[K.item].slot];
+        if (npeel > 0)
+            peel_jobs<true>(S, K.ell, scat_peel, K.int_cell, kx0, ky0, kz0, K.x, K.y, K.z, K.L, p, j0, W.jobs, W.jL);
+        if (nmain) W.jobs[j0 + npeel] = make_int2(p, JOB_MAIN);
+        K.peel_j0 = j0;
+        K.peel_n = npeel;
+    }
+    if (p < W.npool && was_live) {
+        K.flags = (K.flags & 1) | (scat_peel ? 2 : 0);
+        K.state = state;
+        W.pk[p] = K;
+    }
+    __syncthreads();
+    if (threadIdx.x < C_N && s_cnt[threadIdx.x]) atomicAdd(P.counters + threadIdx.x, s_cnt[threadIdx.x]);
+}
+
+// ---------------------------------------------------------------------------------------------
+// traversal pass
+
+// End of the packet's own path (simulateescapeandabsorption :441-462, the termination test of
+// dostellaremissionchunk :283, simulatepropagation :513-531).  Returns 1 when the path must be
+// re-walked to tau_int, 0 when the packet record is complete, -1 on an error.
+__device__ __noinline__ int after_path(const WaveParams& W, const DevScene& S, int p, int phase, int ell,
+                                       double taupath, double Lsca, double& L, double& tau_int) {
+    Packet& K = W.pk[p];
+    if (taupath < 0.0 || isnan(taupath) || isinf(taupath)) {   // DustSystem.cpp:953-955
+        atomicOr(W.R.err, ERR_NAN_TAU);
+        K.state = PK_TERM;
+        return -1;
+    }
+    if (S.ncomp == 1) L = L * S.albedo[ell] * (-expm1(-taupath));
+    else L = Lsca;
+    if (L <= 0 || (L <= K.Lth && K.nscatt >= S.min_scatt_events)) { K.state = PK_TERM; return 0; }
+    if (K.nscatt >= W.R.max_scatt) {
+        atomicOr(W.R.err, ERR_SCATT_BUDGET);
+        K.state = PK_TERM;
+        return -1;
+    }
+    if (taupath == 0.0) {                 // no dust ahead: scatter where the packet is
+        K.L = L; K.s_int = 0; K.int_cell = K.pos_cell >= 0 ? K.pos_cell : -1; K.state = PK_INTERACT;
+        return 0;
+    }
+    const WorkItem& It = W.R.items[K.item];
+    Philox rng;
+    rng.init(It.seed, K.id, (uint32_t)ell | ((uint32_t)phase << 24));
+    rng.c0 = K.rngc;
+    tau_int = sample_interaction(S.xi, taupath, L, rng);
+    K.rngc = rng.c0;
+    return 1;
+}
+
 template<typename R, template<typename> class Stepper>
-__global__ void __launch_bounds__(256, SKG_TRACER_MIN_BLOCKS)
-tracer_kernel(const RunParams P) {
+__global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const WaveParams W) {
     extern __shared__ unsigned char smem_raw[];
     DevGrid* sg = reinterpret_cast<DevGrid*>(smem_raw);
     __shared__ const DevScene* s_scene[MAX_SLOTS];
     __shared__ unsigned long long s_cnt[C_N];
+    const RunParams& P = W.R;
     const BatchHeader H = *P.hdr;
     for (int i = threadIdx.x; i < C_N; i += blockDim.x) s_cnt[i] = 0;
     for (int i = threadIdx.x; i < H.nslots; i += blockDim.x) { sg[i] = P.grids[i]; s_scene[i] = P.scenes[i]; }
     __syncthreads();
-
-    const int lane = threadIdx.x & 31;
+    const unsigned njobs = *W.jcount;
     const int phase = H.phase;
-    const bool peel_on = phase != SKG_PHASE_DUST_SELFABS;
+    const int lane = threadIdx.x & 31;
 
-    Philox rng;
-    int slot = 0;
-    double L = 0, Lth = 0, Lpeel = 0, Lsca_acc = 0;
-    int ell = 0, nscatt = 0, grp = 0;
-    bool stellar = true, scat_peel = false;
-    V3<R> r = mk3((R)0, (R)0, (R)0), k = mk3((R)0, (R)0, (R)1);
-    int mode = M_FETCH, trav = T_NONE;
-    int int_cell = -1;
-    int pos_cell = -2;          // cell holding the packet position: -2 unknown, -1 outside the grid
-    uint64_t Npp_total = 1;
-    double tau = 0, s = 0, tau_int = 0, s_int = 0;
+    int j = -1;                       // the lane's job (-1: none)
+    int p = 0, slot = 0, ell = 0;
+    int kind = 0;                     // 0 peel-off, 1 path, 2 re-walk to the interaction point
+    double tau = 0, s = 0, tau_int = 0, L = 0, Lsca = 0;
     Stepper<R> st;
     unsigned c_steps = 0;
 
     while (true) {
-        // ---------------- event processing: runs until a traversal starts or no work is left.
-        // A lane whose traversal ended waits (idle in the step below) until SKG_EVENT_LANES lanes
-        // of the warp, or all of its live lanes, are waiting, so that the divergent event code is
-        // paid once for many lanes instead of once per finished traversal.
+        // lanes without a job take the next ones: one atomic per warp
         const unsigned live = __activemask();
-        const unsigned waiting = __ballot_sync(live, trav == T_NONE);
-        const bool run_events = __popc(waiting) >= SKG_EVENT_LANES || waiting == live;
-        while (run_events && trav == T_NONE && mode != M_DONE) {
-            const DevGrid& g = sg[slot];
-            const DevScene& S = *s_scene[slot];
-            switch (mode) {
-            case M_FETCH: {
-                unsigned mask = __activemask();
-                int leader = __ffs(mask) - 1;
-                unsigned long long base = 0;
-                if (lane == leader) base = atomicAdd(P.work, (unsigned long long)__popc(mask));
-                base = __shfl_sync(mask, base, leader);
-                uint64_t p = base + __popc(mask & ((1u << lane) - 1));
-                if (p >= H.total) { mode = M_DONE; break; }
-                int it = find_item(P.items, H.nitems, p);
-                const WorkItem W = P.items[it];
-                uint64_t q = p - W.begin;
-                int ei = (int)(q / W.count);
-                uint64_t ip = W.first + (q - (uint64_t)ei * W.count);
-                slot = W.slot;
-                ell = P.ells[W.ell0 + ei];
-                Npp_total = W.npp_total;
-                rng.init(W.seed, ip, (uint32_t)ell | ((uint32_t)phase << 24));
-                atomicAdd(&s_cnt[C_PACKETS], 1ull);
-                mode = M_LAUNCH;        // the launch runs with the packet's own slot bound
-                break;
-            }
-            case M_LAUNCH: {
-                Launched o = launch_packet(g, S, phase, ell, Npp_total, rng);
-                if (!o.ok) { mode = M_FETCH; break; }
-                L = o.L; Lth = o.Lth; stellar = o.stellar;
-                r = mk3((R)o.x, (R)o.y, (R)o.z);
-                k = mk3((R)o.kx, (R)o.ky, (R)o.kz);
-                nscatt = 0; pos_cell = -2; int_cell = -1;
-                if (peel_on) { mode = M_PEEL_NEXT; grp = 0; scat_peel = false; }
-                else mode = M_MAIN1_START;
-                break;
-            }
-            case M_PEEL_NEXT: {
-                // one traversal per direction group (MonteCarloSimulation.cpp:299-357)
-                while (grp < S.ngroups) {
-                    double w = 1.0;
-                    if (scat_peel) {
-                        w = peel_weight(S, ell, int_cell, (double)k.x, (double)k.y, (double)k.z, S.gkx[grp], S.gky[grp],
-                                        S.gkz[grp]);
-                        if (w < 0) { grp = S.ngroups; break; }   // abort peel-off
-                    }
-                    Lpeel = L * w;
-                    if (group_needs_traversal(S, grp, (double)r.x, (double)r.y, (double)r.z)) {
-                        st.init(g, r.x, r.y, r.z, (R)S.gkx[grp], (R)S.gky[grp], (R)S.gkz[grp], pos_cell);
-                        if (pos_cell == -2) pos_cell = st.cell0;
-                        trav = T_PEEL; tau = 0;
-                        break;
-                    }
-                    grp++;
-                }
-                if (trav == T_NONE) mode = scat_peel ? M_SCATTER : M_MAIN1_START;
-                break;
-            }
-            case M_MAIN1_START: {
-                if (S.ncomp == 0) { mode = M_FETCH; break; }
-                st.init(g, r.x, r.y, r.z, k.x, k.y, k.z, pos_cell);
-                if (pos_cell == -2) pos_cell = st.cell0;
-                trav = T_MAIN1; tau = 0; Lsca_acc = 0;
-                break;
-            }
-            case M_AFTER_MAIN1: {
-                double taupath = tau;
-                if (taupath < 0.0 || isnan(taupath) || isinf(taupath)) {   // DustSystem.cpp:953-955
-                    atomicOr(P.err, ERR_NAN_TAU); atomicAdd(&s_cnt[C_ERR], 1ull); mode = M_FETCH; break;
-                }
-                if (S.ncomp == 1) L = L * S.albedo[ell] * (-expm1(-taupath));   // :441-462
-                else L = Lsca_acc;
-                if (L <= 0 || (L <= Lth && nscatt >= S.min_scatt_events)) { mode = M_FETCH; break; }
-                if (nscatt >= P.max_scatt) {
-                    atomicOr(P.err, ERR_SCATT_BUDGET); atomicAdd(&s_cnt[C_ERR], 1ull); mode = M_FETCH; break;
-                }
-                if (taupath == 0.0) { s_int = 0; mode = M_AFTER_MAIN2; break; }
-                tau_int = sample_interaction(S.xi, taupath, L, rng);
-                st.init(g, r.x, r.y, r.z, k.x, k.y, k.z, pos_cell);
-                trav = T_MAIN2; tau = 0; s = 0; s_int = -1; int_cell = -1;
-                break;
-            }
-            case M_AFTER_MAIN2: {
-                R si = (R)s_int;
-                r = mk3(r.x + si * k.x, r.y + si * k.y, r.z + si * k.z);   // PhotonPackage::propagate
-                // the interaction point lies in the cell of its segment (verified by the stepper)
-                if (s_int > 0) pos_cell = (int_cell >= 0) ? int_cell : -2;
-                if (peel_on) { mode = M_PEEL_NEXT; grp = 0; scat_peel = true; }
-                else mode = M_SCATTER;
-                break;
-            }
-            case M_SCATTER: {
-                V3<double> kn = scatter_direction(S, ell, int_cell, mk3((double)k.x, (double)k.y, (double)k.z), rng);
-                k = mk3((R)kn.x, (R)kn.y, (R)kn.z);
-                nscatt++;
-                atomicAdd(&s_cnt[C_SCATT], 1ull);
-                mode = M_MAIN1_START;
-                break;
-            }
-            default: break;
+        const bool need = j < 0;
+        const unsigned want = __ballot_sync(live, need);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            unsigned base = 0;
+            if (lane == leader) base = atomicAdd(W.jcount + 1, (unsigned)__popc(want));
+            base = __shfl_sync(live, base, leader);
+            if (need) {
+                const unsigned jj = base + __popc(want & ((1u << lane) - 1));
+                if (jj >= njobs) break;
+                j = (int)jj;
+                const int2 jb = W.jobs[j];
+                p = jb.x;
+                const Packet& K = W.pk[p];
+                ell = K.ell;
+                slot = P.items[K.item].slot;
+                const DevScene& S = *s_scene[slot];
+                const int hint = K.pos_cell;
+                R kx, ky, kz;
+                if (jb.y == JOB_MAIN) { kx = (R)K.kx; ky = (R)K.ky; kz = (R)K.kz; kind = 1; L = K.L; Lsca = 0; }
+                else { kx = (R)S.gkx[jb.y]; ky = (R)S.gky[jb.y]; kz = (R)S.gkz[jb.y]; kind = 0; }
+                st.init(sg[slot], (R)K.x, (R)K.y, (R)K.z, kx, ky, kz, hint);
+                if (kind == 1 && hint == -2) W.pk[p].pos_cell = st.cell0;
+                tau = 0; s = 0;
             }
         }
-        if (mode == M_DONE) break;
-        if (trav == T_NONE) continue;
 
-        // ---------------- one cell step of the current traversal
+        // one cell step
         const DevGrid& g = sg[slot];
         const DevScene& S = *s_scene[slot];
         int m; R ds;
         if (st.next(g, m, ds)) {
             c_steps++;
             // one dust component: the FP32 tree walk carries the cell density in its leaf record
-            double kr = (S.ncomp == 1 && st.rho >= 0.f) ? S.kext[ell] * (double)st.rho : kappa_rho<R>(S, m, ell);
-            double dtau = kr * (double)ds;
-            if (trav == T_PEEL) {
+            const double kr = (S.ncomp == 1 && st.rho >= 0.f) ? S.kext[ell] * (double)st.rho : kappa_rho<R>(S, m, ell);
+            const double dtau = kr * (double)ds;
+            if (kind == 0) {
                 tau += dtau;
-            } else if (trav == T_MAIN1) {
+            } else if (kind == 1) {
                 if (m >= 0) {
                     const bool store = (phase == SKG_PHASE_STELLAR) ? (S.store_abs != 0) : (phase == SKG_PHASE_DUST_SELFABS);
                     if (S.ncomp == 1) {
                         if (store) {
-                            double Lintm = L * exp(-tau) * (-expm1(-dtau));
+                            const double Lintm = L * exp(-tau) * (-expm1(-dtau));
                             double* labs = (phase == SKG_PHASE_STELLAR) ? S.labs_stel : S.labs_dust;
                             atomicAdd(labs + (size_t)m * S.nlambda + ell, (1.0 - S.albedo[ell]) * Lintm);
                             atomicAdd(&s_cnt[C_ABS], 1ull);
@@ -389,12 +508,12 @@ tracer_kernel(const RunParams P) {
                     } else {
                         double ksca = 0, kext = 0;
                         for (int h = 0; h < S.ncomp; h++) {
-                            double rh = rho_load<R>(S, (size_t)h * S.ncells + m);
+                            const double rh = rho_load<R>(S, (size_t)h * S.ncells + m);
                             ksca += rh * S.ksca[h * S.nlambda + ell]; kext += rh * S.kext[h * S.nlambda + ell];
                         }
-                        double alb = (kext > 0.0) ? ksca / kext : 0.0;
-                        double Lintm = L * exp(-tau) * (-expm1(-dtau));
-                        Lsca_acc += alb * Lintm;
+                        const double alb = (kext > 0.0) ? ksca / kext : 0.0;
+                        const double Lintm = L * exp(-tau) * (-expm1(-dtau));
+                        Lsca += alb * Lintm;
                         if (store) {
                             double* labs = (phase == SKG_PHASE_STELLAR) ? S.labs_stel : S.labs_dust;
                             atomicAdd(labs + (size_t)m * S.nlambda + ell, (1.0 - alb) * Lintm);
@@ -403,78 +522,226 @@ tracer_kernel(const RunParams P) {
                     }
                 }
                 tau += dtau;
-            } else {  // T_MAIN2
-                double tn = tau + dtau, sn = s + (double)ds;
+            } else {
+                const double tn = tau + dtau, sn = s + (double)ds;
                 if (tn > tau_int) {
-                    s_int = s + ((tau_int - tau) / (tn - tau)) * (sn - s);
-                    int_cell = m;
-                    trav = T_NONE; mode = M_AFTER_MAIN2;
+                    Packet& K = W.pk[p];
+                    K.L = L;
+                    K.s_int = s + ((tau_int - tau) / (tn - tau)) * (sn - s);
+                    K.int_cell = m;
+                    K.state = PK_INTERACT;
                     atomicAdd(&s_cnt[C_TRAV], 1ull);
                     atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.scanned);
                     atomicAdd(&s_cnt[C_FB], (unsigned long long)st.fallbacks);
-                } else { tau = tn; s = sn; }
+                    j = -1;
+                } else {
+                    tau = tn; s = sn;
+                }
             }
         } else {
-            // traversal ended
+            // the traversal reached the edge of the grid
             atomicAdd(&s_cnt[C_TRAV], 1ull);
             atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.scanned);
             atomicAdd(&s_cnt[C_FB], (unsigned long long)st.fallbacks);
             if (st.steps > g.max_steps) { atomicOr(P.err, ERR_STEP_BUDGET); atomicAdd(&s_cnt[C_ERR], 1ull); }
-            if (trav == T_PEEL) {
-                int adds = detect_group(S, grp, ell, Lpeel, tau, scat_peel ? nscatt + 1 : 0, stellar,
-                                        (double)r.x, (double)r.y, (double)r.z);
-                atomicAdd(&s_cnt[C_PIX], (unsigned long long)adds);
-                atomicAdd(&s_cnt[C_PEEL], 1ull);
-                grp++;
-                mode = M_PEEL_NEXT;
-            } else if (trav == T_MAIN1) {
-                mode = M_AFTER_MAIN1;
+            if (kind == 0) {
+                W.jtau[j] = tau;
+                j = -1;
+            } else if (kind == 1) {
+                const int rc = after_path(W, S, p, phase, ell, tau, Lsca, L, tau_int);
+                if (rc == 1) {
+                    const Packet& K = W.pk[p];
+                    st.init(g, (R)K.x, (R)K.y, (R)K.z, (R)K.kx, (R)K.ky, (R)K.kz, K.pos_cell);
+                    tau = 0; s = 0; kind = 2;
+                } else {
+                    if (rc < 0) atomicAdd(&s_cnt[C_ERR], 1ull);
+                    j = -1;
+                }
             } else {
-                s_int = s;  // DustGridPath::pathlength: tau beyond the last segment -> full length
-                mode = M_AFTER_MAIN2;
+                // DustGridPath::pathlength: an optical depth beyond the last segment gives the full length
+                Packet& K = W.pk[p];
+                K.L = L; K.s_int = s; K.int_cell = -1; K.state = PK_INTERACT;
+                j = -1;
             }
-            trav = T_NONE;
         }
     }
 
     atomicAdd(&s_cnt[C_STEPS], (unsigned long long)c_steps);
     __syncthreads();
-    if (threadIdx.x < C_N) atomicAdd(P.counters + threadIdx.x, s_cnt[threadIdx.x]);
+    if (threadIdx.x < C_N && s_cnt[threadIdx.x]) atomicAdd(P.counters + threadIdx.x, s_cnt[threadIdx.x]);
 }
 
 // ---------------------------------------------------------------------------------------------
+// host side
+
+namespace {
+
 template<typename R, template<typename> class Stepper>
-static cudaError_t launch_one(const RunParams& P, int nslots, int blocks, int threads, cudaStream_t stream) {
-    auto kern = tracer_kernel<R, Stepper>;
-    size_t smem = (size_t)nslots * sizeof(DevGrid);
-    if (blocks <= 0) {
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem);
-        blocks = sms * (per > 0 ? per : 1);
+cudaError_t enqueue_wave(const WaveParams& W, int nslots, int trav_blocks, cudaEvent_t mid, cudaStream_t s) {
+    auto trav = trav_kernel<R, Stepper>;
+    const size_t smem = (size_t)nslots * sizeof(DevGrid);
+    if (trav_blocks <= 0) {
+        static int per = 0, sms = 0;              // resident blocks of this instantiation
+        if (per == 0) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trav, 256, smem);
+            if (per <= 0) per = 1;
+        }
+        trav_blocks = sms * per;
     }
-    kern<<<blocks, threads, smem, stream>>>(P);
+    event_kernel<R><<<(W.npool + 255) / 256, 256, 0, s>>>(W);
+    if (mid) cudaEventRecord(mid, s);
+    trav<<<trav_blocks, 256, smem, s>>>(W);
     return cudaGetLastError();
 }
 
-cudaError_t launch_tracer(int grid_type, bool bookkeeping, const RunParams& P, int nslots, int precision, int blocks,
-                          int threads, cudaStream_t stream) {
-    if (threads <= 0) threads = 256;
-    bool f64 = precision == SKG_PREC_FP64;
+using WaveFn = cudaError_t (*)(const WaveParams&, int, int, cudaEvent_t, cudaStream_t);
+
+WaveFn pick(int grid_type, bool bookkeeping, int precision) {
+    const bool f64 = precision == SKG_PREC_FP64;
     switch (grid_type) {
     case SKG_GRID_CARTESIAN:
-        return f64 ? launch_one<double, CartStepper>(P, nslots, blocks, threads, stream)
-                   : launch_one<float, CartStepper>(P, nslots, blocks, threads, stream);
+        return f64 ? enqueue_wave<double, CartStepper> : enqueue_wave<float, CartStepper>;
     case SKG_GRID_OCTREE:
     case SKG_GRID_BINTREE:
-        if (f64) return launch_one<double, TreeStepper>(P, nslots, blocks, threads, stream);
-        return bookkeeping ? launch_one<float, TreeNodeWalk>(P, nslots, blocks, threads, stream)
-                           : launch_one<float, TreeStepper>(P, nslots, blocks, threads, stream);
+        if (f64) return enqueue_wave<double, TreeStepper>;
+        return bookkeeping ? enqueue_wave<float, TreeNodeWalk> : enqueue_wave<float, TreeStepper>;
     default:
-        return f64 ? launch_one<double, VoronoiStepper>(P, nslots, blocks, threads, stream)
-                   : launch_one<float, VoronoiStepper>(P, nslots, blocks, threads, stream);
+        return f64 ? enqueue_wave<double, VoronoiStepper> : enqueue_wave<float, VoronoiStepper>;
     }
+}
+
+}  // namespace
+
+WaveRunner::~WaveRunner() {
+    for (cudaEvent_t e : ev_) cudaEventDestroy(e);
+    cudaFree(pk_);
+    for (int b = 0; b < 2; b++) { cudaFree(jobs_[b]); cudaFree(jtau_[b]); cudaFree(jL_[b]); }
+    cudaFree(ctr_);
+    if (h_ctr_) cudaFreeHost(h_ctr_);
+    if (copied_) cudaEventDestroy(copied_);
+}
+
+cudaError_t WaveRunner::reserve(size_t pool, int ngroups) {
+    cudaError_t e;
+    if (!ctr_) {
+        if ((e = cudaMalloc(&ctr_, 8 * sizeof(unsigned))) != cudaSuccess) return e;
+        if ((e = cudaMallocHost((void**)&h_ctr_, 8 * sizeof(unsigned))) != cudaSuccess) return e;
+        if ((e = cudaEventCreateWithFlags(&copied_, cudaEventDisableTiming)) != cudaSuccess) return e;
+    }
+    if (pool > cap_pool_) {
+        cudaFree(pk_); pk_ = nullptr; cap_pool_ = 0;
+        if ((e = cudaMalloc(&pk_, pool * sizeof(Packet))) != cudaSuccess) return e;
+        cap_pool_ = pool;
+    }
+    const size_t jobs = pool * (size_t)(ngroups + 1);
+    if (jobs > cap_jobs_) {
+        for (int b = 0; b < 2; b++) {
+            cudaFree(jobs_[b]); cudaFree(jtau_[b]); cudaFree(jL_[b]);
+            jobs_[b] = nullptr; jtau_[b] = nullptr; jL_[b] = nullptr;
+        }
+        cap_jobs_ = 0;
+        for (int b = 0; b < 2; b++) {
+            if ((e = cudaMalloc(&jobs_[b], jobs * sizeof(int2))) != cudaSuccess) return e;
+            if ((e = cudaMalloc(&jtau_[b], jobs * sizeof(double))) != cudaSuccess) return e;
+            if ((e = cudaMalloc(&jL_[b], jobs * sizeof(double))) != cudaSuccess) return e;
+        }
+        cap_jobs_ = jobs;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t WaveRunner::enqueue(int n) {
+    WaveFn fn = pick(grid_type_, bookkeeping_, precision_);
+    cudaError_t e;
+    for (int i = 0; i < n; i++) {
+        const int w = waves_ + i, b = w & 1;
+        WaveParams W;
+        W.R = P_; W.pk = pk_; W.npool = npool_; W.wave = w;
+        W.jobs = jobs_[b]; W.jtau = jtau_[b]; W.jL = jL_[b]; W.jcount = ctr_ + 3 * b;
+        W.pjobs = jobs_[b ^ 1]; W.pjtau = jtau_[b ^ 1]; W.pjL = jL_[b ^ 1];
+        W.last_busy = ctr_ + 6;
+        if ((e = cudaMemsetAsync(ctr_ + 3 * b, 0, 3 * sizeof(unsigned), stream_)) != cudaSuccess) return e;
+        if (timed_) {
+            while (ev_.size() < 3 * (size_t)(w + 1)) {
+                cudaEvent_t x;
+                if ((e = cudaEventCreate(&x)) != cudaSuccess) return e;
+                ev_.push_back(x);
+            }
+            if ((e = cudaEventRecord(ev_[3 * w], stream_)) != cudaSuccess) return e;
+        }
+        if ((e = fn(W, nslots_, trav_blocks_, timed_ ? ev_[3 * w + 1] : nullptr, stream_)) != cudaSuccess) return e;
+        if (timed_ && (e = cudaEventRecord(ev_[3 * w + 2], stream_)) != cudaSuccess) return e;
+    }
+    waves_ += n;
+    if ((e = cudaMemcpyAsync(h_ctr_, ctr_, 8 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream_)) != cudaSuccess) return e;
+    // inside stream capture the record must become a graph node that the host can wait on
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if ((e = cudaStreamIsCapturing(stream_, &cs)) != cudaSuccess) return e;
+    return cs == cudaStreamCaptureStatusNone ? cudaEventRecord(copied_, stream_)
+                                             : cudaEventRecordWithFlags(copied_, stream_, cudaEventRecordExternal);
+}
+
+cudaError_t WaveRunner::begin(const RunParams& P, int grid_type, bool bookkeeping, int precision, int nslots,
+                              size_t npool, int trav_blocks, cudaStream_t s) {
+    if (npool == 0 || npool > cap_pool_) return cudaErrorInvalidValue;
+    P_ = P; grid_type_ = grid_type; bookkeeping_ = bookkeeping; precision_ = precision; nslots_ = nslots;
+    trav_blocks_ = trav_blocks; stream_ = s; npool_ = (int)npool; waves_ = 0;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cs);
+    timed_ = timing && cs == cudaStreamCaptureStatusNone;
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(pk_, 0, npool * sizeof(Packet), s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(ctr_, 0, 8 * sizeof(unsigned), s)) != cudaSuccess) return e;
+    pending_ = true;
+    return enqueue(estimate);
+}
+
+cudaError_t WaveRunner::finish(int timeout_ms, cudaEvent_t end, bool* timed_out) {
+    if (timed_out) *timed_out = false;
+    const auto t0 = std::chrono::steady_clock::now();
+    bool more = false;                            // waves were added after the caller's end event
+    while (pending_) {
+        while (true) {
+            const cudaError_t q = cudaEventQuery(copied_);
+            if (q == cudaSuccess) break;
+            if (q != cudaErrorNotReady) return q;
+            if (timeout_ms >= 0 &&
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() > timeout_ms) {
+                if (timed_out) *timed_out = true;
+                return cudaSuccess;
+            }
+            std::this_thread::sleep_for(std::chrono::microseconds(50));
+        }
+        const unsigned busy = h_ctr_[3 * ((waves_ - 1) & 1) + 2];
+        if (busy == 0) {
+            pending_ = false;
+            estimate = (int)h_ctr_[6] + 3;        // the last busy wave, the detection wave, one spare
+            break;
+        }
+        cudaError_t e = enqueue(estimate > 32 ? estimate / 4 : 8);
+        if (e != cudaSuccess) { pending_ = false; return e; }
+        more = true;
+    }
+    return (end && more) ? cudaEventRecord(end, stream_) : cudaSuccess;
+}
+
+cudaError_t WaveRunner::times(float* event_ms, float* trav_ms) const {
+    float a = 0, t = 0;
+    if (timed_ && !pending_) {
+        for (int w = 0; w < waves_; w++) {
+            float x = 0, y = 0;
+            cudaError_t e = cudaEventElapsedTime(&x, ev_[3 * w], ev_[3 * w + 1]);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&y, ev_[3 * w + 1], ev_[3 * w + 2]);
+            if (e != cudaSuccess) return e;
+            a += x; t += y;
+        }
+    }
+    if (event_ms) *event_ms = a;
+    if (trav_ms) *trav_ms = t;
+    return cudaSuccess;
 }
 
 }  // namespace skg

@@ -1,0 +1,69 @@
+// skg_wave.h -- host side of the wavefront packet tracer (kernels in skg_tracer.cu).
+//
+// A phase runs as a sequence of waves on one stream.  Wave w: an event pass over the packet pool
+// (detect the previous wave's peel-offs, launch new packets into free records, move scattered
+// packets to their interaction point, scatter, and write the next traversals as jobs) followed by
+// a traversal pass that walks every job of the wave.  The number of waves is not known in
+// advance: begin() enqueues an estimate, finish() reads how many packets still had work after the
+// last enqueued wave and enqueues more until none has.
+#pragma once
+#include "skg_scene.cuh"
+
+#include <vector>
+
+namespace skg {
+
+class WaveRunner {
+public:
+    WaveRunner() = default;
+    WaveRunner(const WaveRunner&) = delete;
+    WaveRunner& operator=(const WaveRunner&) = delete;
+    ~WaveRunner();
+
+    // Sizes the pool and job buffers (allocates; call outside stream capture).  pool packets,
+    // ngroups peel-off groups at most per packet.
+    cudaError_t reserve(size_t pool, int ngroups);
+    // Enqueues the reset of the pool and the first waves of a phase on stream s.  P holds the
+    // staged tables; nslots the slots whose DevGrid the traversal pass keeps in shared memory.
+    cudaError_t begin(const RunParams& P, int grid_type, bool bookkeeping, int precision, int nslots,
+                      size_t npool, int trav_blocks, cudaStream_t s);
+    // Waits for the enqueued waves and enqueues more until no packet is left; then records
+    // `end` (if given) on the phase's stream.  timeout_ms < 0 waits without limit.
+    cudaError_t finish(int timeout_ms, cudaEvent_t end, bool* timed_out);
+    // A captured begin() (pool reset and n waves) was launched as a graph on stream s.
+    void replayed(cudaStream_t s, int n) { pending_ = true; stream_ = s; waves_ = n; }
+    bool pending() const { return pending_; }
+    int waves() const { return waves_; }
+    size_t pool_capacity() const { return cap_pool_; }
+    // With timing on, each wave's two kernels are bracketed by events (not inside graph capture).
+    bool timing = false;
+    // Device time of the finished phase's event passes and traversal passes (ms).
+    cudaError_t times(float* event_ms, float* trav_ms) const;
+
+    int estimate = 24;                // waves the next phase enqueues up front
+
+private:
+    cudaError_t enqueue(int n);
+
+    Packet* pk_ = nullptr;
+    size_t cap_pool_ = 0;
+    int2* jobs_[2] = {nullptr, nullptr};
+    double* jtau_[2] = {nullptr, nullptr};
+    double* jL_[2] = {nullptr, nullptr};
+    size_t cap_jobs_ = 0;
+    unsigned* ctr_ = nullptr;         // [3b .. 3b+2]: counters of job buffer b; [6]: last busy wave
+    unsigned* h_ctr_ = nullptr;       // pinned copy read by finish()
+    cudaEvent_t copied_ = nullptr;
+
+    bool pending_ = false;
+    cudaStream_t stream_ = nullptr;
+    RunParams P_{};
+    int grid_type_ = 0, precision_ = 0, nslots_ = 1, trav_blocks_ = 0;
+    bool bookkeeping_ = false;
+    int npool_ = 0;
+    int waves_ = 0;
+    std::vector<cudaEvent_t> ev_;      // 3 per wave: before the event pass, between, after the traversal
+    bool timed_ = false;               // the running phase records ev_
+};
+
+}  // namespace skg

@@ -94,9 +94,10 @@ class Context:
 
     # ---- the packet loop
     def run_phase(self, phase, ells, npp, first=0, count=None, seed=4357, precision=A.PREC_FP32,
-                  max_steps=0, max_scatt=0, blocks=0, threads=0, stream=None):
+                  max_steps=0, max_scatt=0, blocks=0, pool=0, stream=None):
+        """skg_run_phase.  pool: packets in flight per wave (0 = the library's default)."""
         ells = np.ascontiguousarray(ells, dtype=np.int32)
-        opts = A.RunOpts(precision, max_steps, max_scatt, blocks, threads, 1)
+        opts = A.RunOpts(precision, max_steps, max_scatt, blocks, 0, 1, pool)
         count = npp if count is None else count
         self._ck(self.lib.skg_run_phase(self.h, phase, ells.ctypes.data_as(A.i32p), len(ells), int(npp), int(first),
                                         int(count), int(seed), C.byref(opts), stream))
@@ -108,6 +109,12 @@ class Context:
         ms = C.c_float()
         self._ck(self.lib.skg_last_phase_ms(self.h, C.byref(ms)))
         return ms.value
+
+    def phase_times(self):
+        """(event_ms, traversal_ms, waves) of the last phase: summed device time of its two kernels."""
+        a, b, w = C.c_float(), C.c_float(), C.c_int32()
+        self._ck(self.lib.skg_phase_times(self.h, C.byref(a), C.byref(b), C.byref(w)))
+        return a.value, b.value, w.value
 
     def reset_tallies(self):
         self._ck(self.lib.skg_reset_tallies(self.h))
@@ -176,7 +183,7 @@ class Batch:
         self.h = h
         self._keep = []
 
-    def run(self, phase, slices, precision=A.PREC_FP32, graph=False, stream=None, max_scatt=0):
+    def run(self, phase, slices, precision=A.PREC_FP32, graph=False, stream=None, max_scatt=0, pool=0):
         """slices: list of (Context, ells, npp, first, count, seed)."""
         n = len(slices)
         arr = (A.Work * max(n, 1))()
@@ -185,7 +192,7 @@ class Batch:
             e = np.ascontiguousarray(ells, dtype=np.int32)
             keep.append(e)
             arr[i] = A.Work(ctx.h.value, e.ctypes.data_as(A.i32p), len(e), int(npp), int(first), int(count), int(seed))
-        opts = A.RunOpts(precision, 0, max_scatt, 0, 0, 1)
+        opts = A.RunOpts(precision, 0, max_scatt, 0, 0, 1, pool)
         A.check(self.lib.skg_batch_run(self.h, phase, arr, n, C.byref(opts), A.BATCH_GRAPH if graph else 0, stream))
         self._keep = keep
 

@@ -1,0 +1,204 @@
+"""A request loop for FitSKIRT-style parameter variants: continuous batching on one device.
+
+FitSKIRT evaluates many variants of one ski file, each with a few parameters substituted
+(AdjustableSkirtSimulation.cpp:145-194), and waits for each variant's frames.  Here the variants
+arrive as requests; the loop
+
+  * admits an arrived request as soon as a batch slot is free and its context fits the device
+    memory budget (the context's grid, densities and frames stay resident until its result is
+    read: admission by HBM footprint);
+  * runs *ticks*: one batched launch that carries, for every admitted request, the next slice of
+    its packets (skg_batch_run with one work item per request), so requests that arrive while
+    others are on the device join at the next tick and their work overlaps on the device;
+  * retires a request when its last slice has run: its frames are read and its context freed.
+
+A request's packets carry the same numbers whichever tick runs them (the packet RNG is keyed by
+the request's seed and the packet's index), so its result is the same alone and in the mix, up
+to the summation order of the FP64 tally atomics.
+"""
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi as A
+from . import models, runtime
+from .scene import DEG, KPC, MICRON
+
+
+@dataclass
+class Request:
+    """One variant: (h_R, h_z, tau_V, inclination, bulge fraction), grid size N^3, packets per
+    wavelength, and its arrival time (s, relative to the start of the run)."""
+    rid: int
+    params: tuple
+    N: int
+    packets: int
+    arrival: float
+    seed: int = 0
+    # filled in by the server
+    admitted: float = math.nan
+    done: float = math.nan
+    ticks: int = 0
+    frame: np.ndarray = None
+    _ctx: object = field(default=None, repr=False)
+    _next: int = 0                 # first packet of the next slice
+    _reserved: int = 0             # device bytes reserved at admission
+
+    @property
+    def latency(self):
+        return self.done - self.arrival
+
+
+def fitskirt_requests(n=256, rate=20.0, seed=12345, packets=(1e5, 1e7), grid=(32, 128)):
+    """The variant stream of a fit: parameters uniform in the fit ranges (dust h_R 3-9 kpc, h_z
+    0.1-0.5 kpc, tau_V 0.2-4, inclination 80-90 deg, bulge fraction 0-0.5), Cartesian N^3 with N
+    uniform in `grid`, packets per wavelength log-uniform in `packets`, Poisson arrivals at `rate`
+    per second."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n)) if rate > 0 else np.zeros(n)
+    out = []
+    for i in range(n):
+        p = (rng.uniform(3, 9) * KPC, rng.uniform(0.1, 0.5) * KPC, rng.uniform(0.2, 4.0),
+             rng.uniform(80, 90) * DEG, rng.uniform(0.0, 0.5))
+        N = int(rng.integers(grid[0], grid[1] + 1))
+        npk = int(round(math.exp(rng.uniform(math.log(packets[0]), math.log(packets[1])))))
+        out.append(Request(i, p, N, npk, float(t[i]), seed=1000 + i))
+    return out
+
+
+def build_model(req, npix=256):
+    return models.fit_variant(req.params, req.N, npix=npix)
+
+
+class Server:
+    """Continuous batching over skg_batch on one device.
+
+    hbm_budget   bytes of device memory the admitted contexts may hold together
+    max_slots    simulations per launch (skg_batch slots)
+    tick_packets packets per wavelength a request runs per tick at most; smaller ticks let
+                 arrivals join sooner, larger ones amortise the launch
+    """
+
+    def __init__(self, device=0, hbm_budget=40 << 30, max_slots=64, tick_packets=1 << 20, npix=256,
+                 precision=A.PREC_FP32):
+        self.device = device
+        self.budget = hbm_budget
+        self.max_slots = max_slots
+        self.tick_packets = int(tick_packets)
+        self.npix = npix
+        self.precision = precision
+        self.batch = runtime.Batch(device=device, max_slots=max_slots, max_items=max_slots, max_ells=3 * max_slots)
+        self.reserved = 0            # footprint bounds of the resident contexts (admission)
+        self.in_use = 0              # their actual device bytes
+        self.resident = 0            # resident contexts
+        self.peak_resident = 0
+        self.peak_in_use = 0
+        self.ticks = 0
+
+    def close(self):
+        self.batch.close()
+
+    def _admit(self, req, now):
+        m = build_model(req, self.npix)
+        ctx = runtime.Context(m, device=self.device)
+        req._ctx = ctx
+        req._next = 0
+        req.admitted = now
+        req._reserved = _footprint(req, self.npix)
+        self.reserved += req._reserved
+        self.in_use += ctx.device_bytes
+        self.resident += 1
+        self.peak_resident = max(self.peak_resident, self.resident)
+        self.peak_in_use = max(self.peak_in_use, self.in_use)
+
+    def _retire(self, req, now):
+        ctx = req._ctx
+        cube, _ = ctx.read_instrument(0)
+        req.frame = cube[0]
+        req.done = now
+        self.in_use -= ctx.device_bytes
+        self.reserved -= req._reserved
+        self.resident -= 1
+        ctx.close()
+        req._ctx = None
+
+    def serve(self, requests, realtime=True, on_tick=None):
+        """Runs the request stream to completion; returns the requests with their results and
+        timings.  realtime: arrivals follow the wall clock (else all are present at t=0)."""
+        pending = sorted(requests, key=lambda r: r.arrival)
+        active = []          # in the running tick
+        joining = []         # admitted while a tick runs: they join the next one
+        finished = []
+        t0 = time.perf_counter()
+        i = 0
+
+        def admit(now, n_on_device):
+            nonlocal i
+            while i < len(pending) and (not realtime or pending[i].arrival <= now) and n_on_device < self.max_slots:
+                if n_on_device and self.reserved + _footprint(pending[i], self.npix) > self.budget:
+                    break
+                self._admit(pending[i], now)
+                joining.append(pending[i])
+                n_on_device += 1
+                i += 1
+
+        while i < len(pending) or active or joining:
+            active += joining
+            joining.clear()
+            if not active:
+                now = time.perf_counter() - t0
+                admit(now, 0)
+                if not joining and i < len(pending):
+                    time.sleep(max(0.0, min(0.01, pending[i].arrival - now)))
+                continue
+            # one tick: the next slice of every admitted request in one batched launch
+            slices = []
+            for r in active:
+                cnt = min(self.tick_packets, r.packets - r._next)
+                slices.append((r._ctx, [0, 1, 2], r.packets, r._next, cnt, r.seed))
+            self.batch.run(A.PHASE_STELLAR, slices, precision=self.precision)
+            # arrivals are admitted (contexts built on their own streams) while the tick runs
+            admit(time.perf_counter() - t0, len(active))
+            self.batch.sync()
+            self.ticks += 1
+            now = time.perf_counter() - t0
+            still = []
+            for r in active:
+                r._next += min(self.tick_packets, r.packets - r._next)
+                r.ticks += 1
+                if r._next >= r.packets:
+                    self._retire(r, time.perf_counter() - t0)
+                    finished.append(r)
+                else:
+                    still.append(r)
+            active = still
+            if on_tick:
+                on_tick(self, now)
+        return finished
+
+
+def _footprint(req, npix):
+    """Device bytes of a variant's context, bounded from above before creating it: densities (FP64
+    and FP32) with room for the set-up tables, the Cartesian planes, the frame cube (3 wavelengths)
+    and a fixed allowance for the remaining tables."""
+    nc = req.N ** 3
+    return nc * 24 + 3 * (req.N + 1) * 12 + 3 * npix * npix * 8 + (4 << 20)
+
+
+def run_alone(req, device=0, npix=256, precision=A.PREC_FP32):
+    """The plain single-simulation GPU path for one request: create, run one phase, read the frame.
+    Returns (frame, seconds)."""
+    t0 = time.perf_counter()
+    ctx = runtime.Context(build_model(req, npix), device=device)
+    ctx.run_phase(A.PHASE_STELLAR, [0, 1, 2], req.packets, 0, req.packets, seed=req.seed, precision=precision)
+    cube, _ = ctx.read_instrument(0)
+    ctx.close()
+    return cube[0], time.perf_counter() - t0
+
+
+def latency_stats(reqs):
+    lat = np.array([r.latency for r in reqs])
+    return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "max_s": float(lat.max()), "n": len(lat)}

@@ -48,12 +48,15 @@ def test_dust_emission_matches_oracle(orc):
     G = [gpu_run(m, 40000, 100 + 10 * b) for b in range(12)]
     O = []
     for b in range(12):
-        r = orc.simulate(m, 2000, nthreads=8, seed=500 + b, selfabs_cycles=1, dust_emission_phase=True)
+        r = orc.simulate(m, 4000, nthreads=8, seed=500 + b, selfabs_cycles=1, dust_emission_phase=True)
         O.append(dict(cube=r["cubes"][0][0], ls=r["labs_stel"], ld=r["labs_dust"], T=r["T"]))
     assert all(g["c"]["errors"] == 0 for g in G)
-    # stellar absorption per wavelength (summed over cells) and dust self-absorption
+    # stellar absorption per wavelength (summed over cells) and dust self-absorption.  The standard
+    # errors come from 12 batches a side (about 15 degrees of freedom, heavier tails than a normal
+    # z), and the oracle batches carry a few percent of noise each: bound the largest of the 16
+    # |z| by 5 and their median by 1.5
     z, ok = zscores([g["ls"].sum(0) for g in G], [o["ls"].sum(0) for o in O])
-    assert np.max(np.abs(z[ok])) < 4.5, z
+    assert np.max(np.abs(z[ok])) < 5.0 and np.median(np.abs(z[ok])) < 1.5, z
     z, ok = zscores([g["ld"].sum() for g in G], [o["ld"].sum() for o in O])
     assert abs(float(z)) < 4.0, z
     # equilibrium temperatures of the cells holding most of the dust

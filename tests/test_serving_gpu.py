@@ -1,0 +1,39 @@
+"""The continuous-batching request loop: variants that arrive while others run join at the next
+tick, run their packets in slices spread over several batched launches, and still give the frame
+they give alone (same packets, same numbers; only the summation order of the FP64 atomics
+differs).  Admission respects the slot count and the memory budget."""
+import numpy as np
+import pytest
+
+from skirt7_b200 import serving
+
+pytestmark = pytest.mark.gpu
+
+
+def test_each_result_is_the_same_alone_and_in_the_mix():
+    reqs = serving.fitskirt_requests(n=10, rate=0.0, seed=7, packets=(2e4, 2e5), grid=(24, 40))
+    srv = serving.Server(max_slots=4, tick_packets=30000, npix=64)
+    done = srv.serve(reqs, realtime=False)
+    srv.close()
+    assert len(done) == len(reqs)
+    assert srv.ticks > max(r.ticks for r in done)          # requests overlapped and joined late
+    assert any(r.ticks > 1 for r in done)
+    assert max(r.admitted for r in done) > 0                 # some were admitted after the first tick
+    for r in done[:5]:
+        alone, _ = serving.run_alone(r, npix=64)
+        assert alone.sum() > 0
+        assert np.allclose(r.frame, alone, rtol=1e-10, atol=1e-12 * alone.max()), r.rid
+    st = serving.latency_stats(done)
+    assert st["p50_s"] <= st["p99_s"] and st["n"] == len(reqs)
+
+
+def test_admission_by_memory_budget():
+    reqs = serving.fitskirt_requests(n=6, rate=0.0, seed=8, packets=(2e4, 4e4), grid=(48, 48))
+    est = serving._footprint(reqs[0], 64)
+    srv = serving.Server(max_slots=8, tick_packets=1 << 20, npix=64, hbm_budget=int(2.5 * est))
+    done = srv.serve(reqs, realtime=False)
+    srv.close()
+    assert len(done) == len(reqs)
+    # two 48^3 variants fit the budget, three do not; the bound holds for the real footprint
+    assert srv.peak_resident == 2
+    assert srv.peak_in_use <= 2 * est <= srv.budget
