@@ -41,6 +41,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target duration of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--tree-cache", default=os.path.join(ROOT, "_work", "octree_cache.npz"))
+    p.add_argument("--serving", type=int, default=64,
+                   help="requests of the fit-variant serving leg (Poisson 20/s; 0 = skip)")
     return p.parse_args()
 
 
@@ -314,6 +316,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, model, tree, ctx)
+    srv = serving_leg(args, local) if (rank == 0 and world == 1 and args.serving > 0) else None
 
     if rank == 0:
         line = {
@@ -337,10 +340,39 @@ def main():
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if srv:
+            line["serving"] = srv
         print(json.dumps(line))
     ctx.close()
     if dist:
         dist.destroy_process_group()
+
+
+def serving_leg(args, device):
+    """Fit-variant requests (oligochromatic disk, 3 wavelengths, Cartesian N^3 with N in 32..128,
+    packets per wavelength log-uniform in 1e5..1e7, one 256x256 frame) arriving as a Poisson stream
+    at 20/s, served by continuous batching; then every request alone on the idle device (the plain
+    single-simulation path).  Latency = result in host memory minus arrival."""
+    from skirt7_b200 import serving
+    reqs = serving.fitskirt_requests(n=args.serving, rate=20.0, seed=2024)
+    srv = serving.Server(device=device, max_slots=64, tick_packets=1 << 19, npix=256)
+    t0 = time.perf_counter()
+    done = srv.serve(reqs, realtime=True)
+    wall = time.perf_counter() - t0
+    srv.close()
+    st = serving.latency_stats(done)
+    alone = []
+    for r in reqs:
+        _, sec = serving.run_alone(r, device=device, npix=256)
+        alone.append(sec)
+    alone = sorted(alone)
+    import numpy as np
+    a50, a99 = float(np.percentile(alone, 50)), float(np.percentile(alone, 99))
+    packets = sum(3 * r.packets for r in reqs)
+    return {"requests": len(reqs), "arrival_rate_per_s": 20.0, "p50_s": st["p50_s"], "p99_s": st["p99_s"],
+            "alone_p50_s": a50, "alone_p99_s": a99, "p99_over_alone_p99": st["p99_s"] / a99,
+            "packets_per_s": packets / wall, "makespan_s": wall, "ticks": srv.ticks,
+            "peak_resident": srv.peak_resident}
 
 
 def cpu_baseline(args, model, tree, ctx):

@@ -214,6 +214,10 @@ struct CartStepper {
     // next segment; false when the path has ended
     SKG_D bool next(const DevGrid& g, int& m, R& ds) {
         if (pd.pop(ds)) { m = -1; return true; }
+        return walk(g, m, ds);
+    }
+    // the segments inside the grid (after the entry segments have been taken)
+    SKG_D bool walk(const DevGrid& g, int& m, R& ds) {
         while (!done) {
             if (++steps > g.max_steps) { done = true; return false; }
             m = k + g.nz * j + g.nz * g.ny * i;
@@ -320,6 +324,10 @@ struct TreeNodeWalk {
 
     SKG_D bool next(const DevGrid& g, int& m, R& ds) {
         if (pd.pop(ds)) { m = -1; return true; }
+        return walk(g, m, ds);
+    }
+    // the segments inside the grid (after the entry segments have been taken)
+    SKG_D bool walk(const DevGrid& g, int& m, R& ds) {
         while (!done) {
             if (++steps > g.max_steps) { done = true; return false; }
             if (g.search == 2) { if (bookkeeping(g, m, ds)) return true; else continue; }
@@ -448,7 +456,7 @@ template<typename R> struct TreeStepper : TreeNodeWalk<R> {};
 template<>
 struct TreeStepper<float> {
     float x, y, z, kx, ky, kz;
-    float4 r0, r1, r2, r3;      // the current leaf's record
+    float4 r0, r1;              // the current leaf's box, density and cell (its ropes stay in L1)
     int leaf;
     Pend<float> pd;
     bool done;
@@ -458,7 +466,7 @@ struct TreeStepper<float> {
 
     SKG_D void load(const DevGrid& g, int li) {
         const float4* p = g.lrec + 4 * (size_t)li;
-        r0 = __ldg(p); r1 = __ldg(p + 1); r2 = __ldg(p + 2); r3 = __ldg(p + 3);
+        r0 = __ldg(p); r1 = __ldg(p + 1);
     }
     SKG_D bool inside(float px, float py, float pz) const {
         return px >= r0.x && px <= r1.x && py >= r0.y && py <= r1.y && pz >= r0.z && pz <= r1.z;
@@ -468,12 +476,13 @@ struct TreeStepper<float> {
     SKG_D static int descend(const DevGrid& g, int ref, float px, float py, float pz) {
         int guard = 0;
         while (ref < -1 && guard++ < 64) {
+            // the split point and both child-reference vectors in one round trip (one 48-byte record)
             const float4* p = g.irec + 3 * (size_t)(-ref - 2);
-            float4 a = __ldg(p);
+            const float4 a = __ldg(p), b0 = __ldg(p + 1), b1 = __ldg(p + 2);
             int d = __float_as_int(a.w), c;
             if (d < 0) c = (px < a.x ? 0 : 1) + (py < a.y ? 0 : 2) + (pz < a.z ? 0 : 4);
             else c = ((d == 0 ? px < a.x : d == 1 ? py < a.y : pz < a.z) ? 0 : 1);
-            float4 b = __ldg(p + 1 + (c >> 2));
+            const float4 b = (c >> 2) ? b1 : b0;
             int k = c & 3;
             ref = __float_as_int(k == 0 ? b.x : k == 1 ? b.y : k == 2 ? b.z : b.w);
         }
@@ -503,6 +512,10 @@ struct TreeStepper<float> {
 
     SKG_D bool next(const DevGrid& g, int& m, float& ds) {
         if (pd.pop(ds)) { m = -1; rho = 0.f; return true; }
+        return walk(g, m, ds);
+    }
+    // the segments inside the grid (after the entry segments have been taken)
+    SKG_D bool walk(const DevGrid& g, int& m, float& ds) {
         const float eps = g.epsf;
         while (!done) {
             if (++steps > g.max_steps) { done = true; return false; }
@@ -512,10 +525,12 @@ struct TreeStepper<float> {
             float dsx = (fabsf(kx) > 1e-15f) ? (xnext - x) / kx : FLT_MAX;
             float dsy = (fabsf(ky) > 1e-15f) ? (ynext - y) / ky : FLT_MAX;
             float dsz = (fabsf(kz) > 1e-15f) ? (znext - z) / kz : FLT_MAX;
-            float d; int rope;
-            if (dsx <= dsy && dsx <= dsz) { d = dsx; rope = __float_as_int((kx < 0.f) ? r2.x : r2.y); }
-            else if (dsy <= dsx && dsy <= dsz) { d = dsy; rope = __float_as_int((ky < 0.f) ? r2.z : r2.w); }
-            else { d = dsz; rope = __float_as_int((kz < 0.f) ? r3.x : r3.y); }
+            float d; int face;          // exit wall: 0..5 = x-, x+, y-, y+, z-, z+
+            if (dsx <= dsy && dsx <= dsz) { d = dsx; face = (kx < 0.f) ? 0 : 1; }
+            else if (dsy <= dsx && dsy <= dsz) { d = dsy; face = (ky < 0.f) ? 2 : 3; }
+            else { d = dsz; face = (kz < 0.f) ? 4 : 5; }
+            // the rope of that wall: words 8..13 of the leaf's record (the line is in L1)
+            const int rope = __ldg(reinterpret_cast<const int*>(g.lrec + 4 * (size_t)leaf + 2) + face);
             m = __float_as_int(r1.w);
             rho = r0.w;
             x += (d + eps) * kx; y += (d + eps) * ky; z += (d + eps) * kz;
@@ -615,13 +630,17 @@ struct VoronoiStepper {
         x = rx; y = ry; z = rz;
     }
 
-    SKG_D bool next(const DevGrid& g, int& m, R& ds);
+    SKG_D bool next(const DevGrid& g, int& m, R& ds) {
+        if (pd.pop(ds)) { m = -1; return true; }
+        return walk(g, m, ds);
+    }
+    // the segments inside the grid (after the entry segments have been taken)
+    SKG_D bool walk(const DevGrid& g, int& m, R& ds);
 };
 
 // FP64: the reference arithmetic on the generator sites (VoronoiMesh.cpp:803-858)
 template<>
-SKG_D bool VoronoiStepper<double>::next(const DevGrid& g, int& m, double& ds) {
-    if (pd.pop(ds)) { m = -1; return true; }
+SKG_D bool VoronoiStepper<double>::walk(const DevGrid& g, int& m, double& ds) {
     while (!done) {
         if (++steps > g.max_steps) { done = true; return false; }
         V3<double> pr = site_pos<double>(g, mr);
@@ -670,8 +689,7 @@ SKG_D bool VoronoiStepper<double>::next(const DevGrid& g, int& m, double& ds) {
 
 // FP32: precomputed bisector planes, one 16-byte load per neighbour entry
 template<>
-SKG_D bool VoronoiStepper<float>::next(const DevGrid& g, int& m, float& ds) {
-    if (pd.pop(ds)) { m = -1; return true; }
+SKG_D bool VoronoiStepper<float>::walk(const DevGrid& g, int& m, float& ds) {
     while (!done) {
         if (++steps > g.max_steps) { done = true; return false; }
         float sq = FLT_MAX;

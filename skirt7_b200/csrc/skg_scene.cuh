@@ -145,11 +145,13 @@ struct WaveParams {
     Packet* pk;
     int npool;
     int wave;                         // index of this wave within the phase
-    // this wave's jobs (written by the event pass, walked by the traversal pass)
+    // this wave's jobs (written by the event pass, walked by the traversal pass): path jobs at
+    // [0, npool) and peel-off jobs from npool on, so that the longest jobs are taken first
     int2* jobs;                       // (packet, type)
     double* jtau;                     // peel-off optical depth
     double* jL;                       // peel-off luminosity
-    unsigned* jcount;                 // [0] jobs, [1] jobs taken by the traversal pass, [2] packets with jobs
+    unsigned* jcount;                 // [0] path jobs, [1] peel-off jobs, [2] jobs taken by the
+                                      // traversal pass, [3] packets with jobs
     // the previous wave's jobs (peel-off detection)
     const int2* pjobs;
     const double* pjtau;

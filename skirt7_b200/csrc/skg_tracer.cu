@@ -38,7 +38,7 @@
 namespace skg {
 
 #ifndef SKG_TRAV_MIN_BLOCKS
-#define SKG_TRAV_MIN_BLOCKS 3
+#define SKG_TRAV_MIN_BLOCKS 4
 #endif
 
 enum Cnt : int { C_PACKETS = 0, C_STEPS, C_TRAV, C_SCATT, C_PEEL, C_ABS, C_PIX, C_NBR, C_FB, C_ERR, C_N };
@@ -363,31 +363,34 @@ __global__ void __launch_bounds__(256) event_kernel(const WaveParams W) {
         }
     }
 
-    // 4. append the jobs: one reservation per warp, each packet's jobs contiguous
-    const int n = npeel + nmain;
-    int incl = n;
+    // 4. append the jobs, one reservation per warp for each kind: the path jobs (the longest)
+    //    from index 0, a packet's peel-off jobs contiguous from index npool on
+    int inm = nmain, inp = npeel;
     for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(FULL, incl, o);
-        if (lane >= o) incl += t;
+        const int tm = __shfl_up_sync(FULL, inm, o), tp = __shfl_up_sync(FULL, inp, o);
+        if (lane >= o) { inm += tm; inp += tp; }
     }
-    const int tot = __shfl_sync(FULL, incl, 31);
-    unsigned base = 0;
-    if (lane == 31 && tot > 0) base = atomicAdd(W.jcount, (unsigned)tot);
-    base = __shfl_sync(FULL, base, 31);
-    const unsigned busy = __ballot_sync(FULL, n > 0);
+    const int totm = __shfl_sync(FULL, inm, 31), totp = __shfl_sync(FULL, inp, 31);
+    unsigned bm = 0, bp = 0;
+    if (lane == 31) {
+        if (totm > 0) bm = atomicAdd(W.jcount, (unsigned)totm);
+        if (totp > 0) bp = atomicAdd(W.jcount + 1, (unsigned)totp);
+    }
+    bm = __shfl_sync(FULL, bm, 31);
+    bp = __shfl_sync(FULL, bp, 31);
+    const unsigned busy = __ballot_sync(FULL, npeel + nmain > 0);
     if (lane == 0 && busy) {
-        atomicAdd(W.jcount + 2, (unsigned)__popc(busy));
+        atomicAdd(W.jcount + 3, (unsigned)__popc(busy));
         atomicMax(W.last_busy, (unsigned)W.wave);
     }
-    if (n > 0) {
-        const int j0 = (int)(base + incl - n);
+    if (npeel > 0) {
+        const int j0 = W.npool + (int)(bp + inp - npeel);
         const DevScene& S = *P.scenes[P.items[K.item].slot];
-        if (npeel > 0)
-            peel_jobs<true>(S, K.ell, scat_peel, K.int_cell, kx0, ky0, kz0, K.x, K.y, K.z, K.L, p, j0, W.jobs, W.jL);
-        if (nmain) W.jobs[j0 + npeel] = make_int2(p, JOB_MAIN);
+        peel_jobs<true>(S, K.ell, scat_peel, K.int_cell, kx0, ky0, kz0, K.x, K.y, K.z, K.L, p, j0, W.jobs, W.jL);
         K.peel_j0 = j0;
-        K.peel_n = npeel;
     }
+    K.peel_n = npeel;
+    if (nmain) W.jobs[bm + inm - 1] = make_int2(p, JOB_MAIN);
     if (p < W.npool && was_live) {
         K.flags = (K.flags & 1) | (scat_peel ? 2 : 0);
         K.state = state;
@@ -443,7 +446,7 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
     for (int i = threadIdx.x; i < C_N; i += blockDim.x) s_cnt[i] = 0;
     for (int i = threadIdx.x; i < H.nslots; i += blockDim.x) { sg[i] = P.grids[i]; s_scene[i] = P.scenes[i]; }
     __syncthreads();
-    const unsigned njobs = *W.jcount;
+    const unsigned nmainj = W.jcount[0], njobs = nmainj + W.jcount[1];
     const int phase = H.phase;
     const int lane = threadIdx.x & 31;
 
@@ -462,12 +465,12 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
         if (want) {
             const int leader = __ffs(want) - 1;
             unsigned base = 0;
-            if (lane == leader) base = atomicAdd(W.jcount + 1, (unsigned)__popc(want));
+            if (lane == leader) base = atomicAdd(W.jcount + 2, (unsigned)__popc(want));
             base = __shfl_sync(live, base, leader);
             if (need) {
                 const unsigned jj = base + __popc(want & ((1u << lane) - 1));
                 if (jj >= njobs) break;
-                j = (int)jj;
+                j = jj < nmainj ? (int)jj : W.npool + (int)(jj - nmainj);
                 const int2 jb = W.jobs[j];
                 p = jb.x;
                 const Packet& K = W.pk[p];
@@ -481,6 +484,10 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
                 st.init(sg[slot], (R)K.x, (R)K.y, (R)K.z, kx, ky, kz, hint);
                 if (kind == 1 && hint == -2) W.pk[p].pos_cell = st.cell0;
                 tau = 0; s = 0;
+                // entry segments outside the grid (m = -1) carry no optical depth: only their
+                // length counts (for the re-walk)
+                R d0;
+                while (st.pd.pop(d0)) s += (double)d0;
             }
         }
 
@@ -488,7 +495,7 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
         const DevGrid& g = sg[slot];
         const DevScene& S = *s_scene[slot];
         int m; R ds;
-        if (st.next(g, m, ds)) {
+        if (st.walk(g, m, ds)) {
             c_steps++;
             // one dust component: the FP32 tree walk carries the cell density in its leaf record
             const double kr = (S.ncomp == 1 && st.rho >= 0.f) ? S.kext[ell] * (double)st.rho : kappa_rho<R>(S, m, ell);
@@ -553,6 +560,8 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
                     const Packet& K = W.pk[p];
                     st.init(g, (R)K.x, (R)K.y, (R)K.z, (R)K.kx, (R)K.ky, (R)K.kz, K.pos_cell);
                     tau = 0; s = 0; kind = 2;
+                    R d0;
+                    while (st.pd.pop(d0)) s += (double)d0;
                 } else {
                     if (rc < 0) atomicAdd(&s_cnt[C_ERR], 1ull);
                     j = -1;
@@ -627,8 +636,8 @@ WaveRunner::~WaveRunner() {
 cudaError_t WaveRunner::reserve(size_t pool, int ngroups) {
     cudaError_t e;
     if (!ctr_) {
-        if ((e = cudaMalloc(&ctr_, 8 * sizeof(unsigned))) != cudaSuccess) return e;
-        if ((e = cudaMallocHost((void**)&h_ctr_, 8 * sizeof(unsigned))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&ctr_, NCTR * sizeof(unsigned))) != cudaSuccess) return e;
+        if ((e = cudaMallocHost((void**)&h_ctr_, NCTR * sizeof(unsigned))) != cudaSuccess) return e;
         if ((e = cudaEventCreateWithFlags(&copied_, cudaEventDisableTiming)) != cudaSuccess) return e;
     }
     if (pool > cap_pool_) {
@@ -660,10 +669,10 @@ cudaError_t WaveRunner::enqueue(int n) {
         const int w = waves_ + i, b = w & 1;
         WaveParams W;
         W.R = P_; W.pk = pk_; W.npool = npool_; W.wave = w;
-        W.jobs = jobs_[b]; W.jtau = jtau_[b]; W.jL = jL_[b]; W.jcount = ctr_ + 3 * b;
+        W.jobs = jobs_[b]; W.jtau = jtau_[b]; W.jL = jL_[b]; W.jcount = ctr_ + 4 * b;
         W.pjobs = jobs_[b ^ 1]; W.pjtau = jtau_[b ^ 1]; W.pjL = jL_[b ^ 1];
-        W.last_busy = ctr_ + 6;
-        if ((e = cudaMemsetAsync(ctr_ + 3 * b, 0, 3 * sizeof(unsigned), stream_)) != cudaSuccess) return e;
+        W.last_busy = ctr_ + 8;
+        if ((e = cudaMemsetAsync(ctr_ + 4 * b, 0, 4 * sizeof(unsigned), stream_)) != cudaSuccess) return e;
         if (timed_) {
             while (ev_.size() < 3 * (size_t)(w + 1)) {
                 cudaEvent_t x;
@@ -676,7 +685,7 @@ cudaError_t WaveRunner::enqueue(int n) {
         if (timed_ && (e = cudaEventRecord(ev_[3 * w + 2], stream_)) != cudaSuccess) return e;
     }
     waves_ += n;
-    if ((e = cudaMemcpyAsync(h_ctr_, ctr_, 8 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream_)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(h_ctr_, ctr_, NCTR * sizeof(unsigned), cudaMemcpyDeviceToHost, stream_)) != cudaSuccess) return e;
     // inside stream capture the record must become a graph node that the host can wait on
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if ((e = cudaStreamIsCapturing(stream_, &cs)) != cudaSuccess) return e;
@@ -694,7 +703,7 @@ cudaError_t WaveRunner::begin(const RunParams& P, int grid_type, bool bookkeepin
     timed_ = timing && cs == cudaStreamCaptureStatusNone;
     cudaError_t e;
     if ((e = cudaMemsetAsync(pk_, 0, npool * sizeof(Packet), s)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(ctr_, 0, 8 * sizeof(unsigned), s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(ctr_, 0, NCTR * sizeof(unsigned), s)) != cudaSuccess) return e;
     pending_ = true;
     return enqueue(estimate);
 }
@@ -715,10 +724,10 @@ cudaError_t WaveRunner::finish(int timeout_ms, cudaEvent_t end, bool* timed_out)
             }
             std::this_thread::sleep_for(std::chrono::microseconds(50));
         }
-        const unsigned busy = h_ctr_[3 * ((waves_ - 1) & 1) + 2];
+        const unsigned busy = h_ctr_[4 * ((waves_ - 1) & 1) + 3];
         if (busy == 0) {
             pending_ = false;
-            estimate = (int)h_ctr_[6] + 3;        // the last busy wave, the detection wave, one spare
+            estimate = (int)h_ctr_[8] + 3;        // the last busy wave, the detection wave, one spare
             break;
         }
         cudaError_t e = enqueue(estimate > 32 ? estimate / 4 : 8);

@@ -259,6 +259,31 @@ def build_tree(model: SceneModel, gtype, extent, minLevel=2, maxLevel=6, maxMass
     return _tree_from_handle(lib, h, gtype, extent, searchMethod)
 
 
+def build_voronoi(sites, extent, device=0):
+    """VoronoiMesh::buildMesh (VoronoiMesh.cpp:297-405) on the device: the tessellation of the
+    generator points inside the domain box, with the block lists of the cell search."""
+    from .scene import VoronoiDustGrid
+    lib = A.load()
+    s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+    h = C.c_void_p()
+    A.check(lib.skg_voronoi_build(s.ctypes.data_as(A.dp), len(s), *[float(v) for v in extent], device, C.byref(h)))
+    try:
+        n, nn, nb, nbid = C.c_int32(), C.c_int64(), C.c_int32(), C.c_int64()
+        A.check(lib.skg_voronoi_sizes(h, C.byref(n), C.byref(nn), C.byref(nb), C.byref(nbid)))
+        n = n.value
+        pos, off = np.zeros((n, 3)), np.zeros(n + 1, dtype=np.int64)
+        ids, vol = np.zeros(nn.value, dtype=np.int32), np.zeros(n)
+        cen, bbox = np.zeros((n, 3)), np.zeros((n, 6))
+        boff, bids = np.zeros(nb.value ** 3 + 1, dtype=np.int64), np.zeros(nbid.value, dtype=np.int32)
+        A.check(lib.skg_voronoi_arrays(h, pos.ctypes.data_as(A.dp), off.ctypes.data_as(A.i64p),
+                                       ids.ctypes.data_as(A.i32p), vol.ctypes.data_as(A.dp), cen.ctypes.data_as(A.dp),
+                                       bbox.ctypes.data_as(A.dp), boff.ctypes.data_as(A.i64p),
+                                       bids.ctypes.data_as(A.i32p)))
+    finally:
+        lib.skg_voronoi_destroy(h)
+    return VoronoiDustGrid(extent, pos, off, ids, nb.value, boff, bids, vol, bbox)
+
+
 def tree_from_splits(gtype, extent, split, searchMethod=A.SEARCH_NEIGHBOR):
     lib = A.load()
     split = np.ascontiguousarray(split, dtype=np.uint8)
