@@ -1,12 +1,20 @@
-"""Benchmark: photon packets/s of SKIRT7's stellar-emission packet loop on the panchromatic octree
-disk galaxy (50 log-spaced wavelengths 0.1-10 micron, octree max level 10 with cell mass fraction
-< 1e-6, three 512x512 frames at 0/60/88 degrees, FP32 geometry with FP64 tallies).
+"""Benchmark: photon packets/s of SKIRT7's packet life cycle on the device.
 
-One step = one stellar-emission phase (a sequence of waves: an event pass and a traversal pass
-each) over all 50 wavelengths with --packets packets per wavelength per GPU.  Ranks (torchrun, one per GPU) run disjoint packet
-ranges of one simulation and all-reduce the frames over NCCL at the end of each step (weak
-scaling: the packets per GPU are fixed).  `value` is device-timed; `e2e` is the same metric
-through the C ABI with the tallies read back into host memory every step.
+Default workload (the headline): the stellar-emission phase of the panchromatic octree disk galaxy
+(50 log-spaced wavelengths 0.1-10 micron, octree max level 10 with cell mass fraction < 1e-6,
+three 512x512 frames at 0/60/88 degrees, FP32 geometry with FP64 tallies).  --workload selects the
+other configurations of the hot path with the same machinery:
+  cartesian_oligo   oligochromatic disk on a 100x100x50 Cartesian grid, 300x300 frame + SED at 88 deg
+  voronoi_clumpy    clumpy dust disk (10^4 clumps, 25 % of the mass) on a 10^6-site Voronoi grid
+  kdtree_dust       panchromatic disk + point source on a k-d tree, 100 wavelengths 0.1-1000 micron,
+                    one step = stellar phase with absorption tallies + dust emission spectra +
+                    dust-emission phase
+
+One step = the workload's phases (a sequence of waves: an event pass and a traversal pass each)
+over all wavelengths with --packets packets per wavelength per GPU.  Ranks (torchrun, one per GPU)
+run disjoint packet ranges of one simulation and all-reduce the frames over NCCL at the end of
+each step (weak scaling: the packets per GPU are fixed).  `value` is device-timed; `e2e` is the
+same metric through the C ABI with the tallies read back into host memory every step.
 
 --impl reference times the reference's algorithm on the host cores: the oracle (a scalar FP64
 restatement of the reference's life cycle, oracle/oracle.cpp) with all host threads on a
@@ -25,6 +33,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 MEASURED = os.path.join(ROOT, "MEASURED_PEAKS.json")
+WORKLOADS = ("octree_pan", "cartesian_oligo", "voronoi_clumpy", "kdtree_dust")
 
 
 def parse():
@@ -33,6 +42,7 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--workload", default="octree_pan", choices=WORKLOADS)
     p.add_argument("--packets", type=float, default=1e6, help="packets per wavelength per GPU per step")
     p.add_argument("--max-level", type=int, default=10)
     p.add_argument("--mass-fraction", type=float, default=1e-6)
@@ -95,13 +105,91 @@ class Clocks:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def build_model(args):
-    from skirt7_b200 import models
-    return models.pan_disk(nlambda=args.nlambda, inclinations=(0, 60, 88), npix=512)
+# ---------------------------------------------------------------------------------------------
+# workloads
+
+class Workload:
+    """A configuration: its scene (grid built on the device), the phases of one step and the
+    algorithmic bytes of its traversal pass."""
+
+    def __init__(self, args, device):
+        from skirt7_b200 import _abi as A
+        from skirt7_b200 import models, runtime
+        from skirt7_b200.scene import KPC
+        self.name = args.workload
+        self.grid_s = 0.0
+        self.dust_phase = False
+        ext = (-20 * KPC, -20 * KPC, -2 * KPC, 20 * KPC, 20 * KPC, 2 * KPC)
+        t0 = time.time()
+        if self.name == "octree_pan":
+            self.model = models.pan_disk(nlambda=args.nlambda, inclinations=(0, 60, 88), npix=512)
+            self.model.dustGrid, self.grid_s = get_tree(args, self.model, device)
+            self.metric = "photon packets/s (stellar emission, octree pan disk)"
+            self.desc = ("panchromatic octree disk galaxy: %d wavelengths 0.1-10 micron, octree max level %d, mass "
+                         "fraction %g (%d leaves), 3 frames 512x512 at 0/60/88 deg" %
+                         (args.nlambda, args.max_level, args.mass_fraction, self.model.dustGrid.ncells))
+        elif self.name == "cartesian_oligo":
+            self.model = models.oligo_disk()
+            self.metric = "photon packets/s (oligochromatic disk, Cartesian grid)"
+            self.desc = ("oligochromatic disk galaxy at 0.55 micron: 100x100x50 Cartesian grid, tau_V 1, "
+                         "300x300 frame + SED at 88 deg")
+        elif self.name == "voronoi_clumpy":
+            import numpy as np
+            self.model = models.clumpy_disk()
+            rng = np.random.default_rng(77)
+            n = 1000000
+            lo, hi = np.array(ext[:3]), np.array(ext[3:])
+            base = self.model.dustComps[0].geometry.geometry
+            d = np.zeros((0, 3))
+            while len(d) < int(0.8 * n):
+                q = models.sample_expdisk(base, n, rng).reshape(-1, 3)
+                d = np.concatenate([d, q[np.all((q > lo) & (q < hi), axis=1)]])
+            sites = np.concatenate([d[: int(0.8 * n)], lo + rng.random((n - int(0.8 * n), 3)) * (hi - lo)])
+            self.model.dustGrid = runtime.build_voronoi(sites, ext, device)
+            self.grid_s = time.time() - t0
+            self.metric = "photon packets/s (clumpy disk, Voronoi grid)"
+            self.desc = ("clumpy dust disk at 0.55 micron (tau_V 5, 10^4 cubic-spline clumps with 25 %% of the "
+                         "mass): Voronoi grid of %d sites (80 %% from the disk density, 20 %% uniform), 300x300 "
+                         "frame at 88 deg" % self.model.dustGrid.ncells)
+        else:
+            self.model = models.pan_disk(nlambda=100, lmin=0.1e-6, lmax=1000e-6, inclinations=(60,), npix=512,
+                                         point_fraction=0.1, dust_emission=True, write_absorption=True)
+            self.model.dustGrid = runtime.build_tree(self.model, A.GRID_BINTREE, ext, minLevel=6, maxLevel=30,
+                                                     maxMassFraction=args.mass_fraction / 2, sampleCount=100,
+                                                     seed=4357, device=device)
+            self.grid_s = time.time() - t0
+            self.dust_phase = True
+            self.metric = "photon packets/s (stellar + dust emission, k-d tree pan disk)"
+            self.desc = ("panchromatic disk + point source (10 %% of L) with grey-body dust emission: k-d tree "
+                         "(alternating, %d leaves), 100 wavelengths 0.1-1000 micron, 512x512 frame at 60 deg; "
+                         "a step is the stellar phase, the dust emission spectra and the dust-emission phase"
+                         % self.model.dustGrid.ncells)
+        self.model.rho = None
+        self.gtype = type(self.model.dustGrid).__name__
+
+    def alg_bytes(self, c, fp32):
+        """Algorithmic bytes of the traversal pass from the exact counters.  Per cell step: tree --
+        the leaf box (24 B) and density (4 B), plus the followed rope (4 B); Cartesian -- the crossed
+        plane (4 B) and the density (4 B); Voronoi -- the density (4 B) plus, per neighbour entry
+        tested, its bisector plane (16 B) and id (4 B).  Per absorption tally 8 B.  The FP64 walk
+        doubles the box, plane and density words."""
+        f = 1 if fp32 else 2
+        if self.gtype == "CartesianDustGrid":
+            b = c["steps"] * 8 * f
+        elif self.gtype == "VoronoiDustGrid":
+            b = c["steps"] * 4 * f + c["nbr_scanned"] * (16 * f + 4)
+        else:
+            b = c["steps"] * 28 * f + c["nbr_scanned"] * 4
+        return b + 8 * c["absorb_adds"]
+
+    def frames(self):
+        from skirt7_b200 import _abi as A
+        return [i for i, ins in enumerate(self.model.instruments) if ins.type != A.INSTR_SED]
 
 
 def get_tree(args, model, device):
-    """The octree of the workload (device-sampled subdivision); cached across runs of the same size."""
+    """The octree of the headline workload (device-sampled subdivision); cached across runs of the
+    same size."""
     import numpy as np
     from skirt7_b200 import _abi as A
     from skirt7_b200 import runtime
@@ -126,40 +214,41 @@ def get_tree(args, model, device):
     return tree, dt
 
 
+# ---------------------------------------------------------------------------------------------
+# the reference arm
+
 def run_reference(args, rank, world):
     """The reference algorithm on the host cores (rank 0 only)."""
     if rank != 0:
         return
+    if not _has_gpu():
+        print(json.dumps({"impl": "reference", "unavailable": "the workload's grid is built on the device; no GPU"}))
+        return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    import numpy as np
-    from skirt7_b200 import _abi as A
-    model = build_model(args)
-    tree, _ = get_tree(args, model, 0) if _has_gpu() else (None, 0)
-    if tree is None:
-        print(json.dumps({"impl": "reference", "unavailable": "the octree is built on the device; no GPU present"}))
-        return
-    model.dustGrid = tree
-    model.rho = _density_for(model, tree)
+    wl = Workload(args, 0)
+    model = wl.model
+    model.rho = _density_for(model)
     threads = os.cpu_count() or 1
     oracle.build()
+    kw = dict(dust_emission_phase=wl.dust_phase)
     # calibrate the sample to about --cpu-seconds per step
-    probe = oracle.simulate(model, args.packets * args.gpus, nthreads=threads, seed=1, max_packets=2000)
+    probe = oracle.simulate(model, args.packets * args.gpus, nthreads=threads, seed=1, max_packets=2000, **kw)
     rate = probe["stats"]["packets"] / max(probe["stats"]["seconds"], 1e-6)
     sample = int(max(1000, min(2e6, rate * args.cpu_seconds)))
     vals = []
     for s in range(args.warmup + args.steps):
-        r = oracle.simulate(model, args.packets * args.gpus, nthreads=threads, seed=100 + s, max_packets=sample)
+        r = oracle.simulate(model, args.packets * args.gpus, nthreads=threads, seed=100 + s, max_packets=sample, **kw)
         if s >= args.warmup:
             vals.append(r["stats"]["packets"] / r["stats"]["seconds"])
     v = statistics.mean(vals)
-    line = {"metric": "photon packets/s (stellar emission, octree pan disk)", "value": v, "unit": "packets/s",
+    line = {"metric": wl.metric, "value": v, "unit": "packets/s",
             "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sample / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": _config(args, tree),
+            "config": _config(args, wl),
             "cpu_baseline": {"value": v, "unit": "packets/s", "cores": threads, "kind": "port",
-                             "sample": "%d packets of the workload (all 50 wavelengths) per step" % sample},
+                             "sample": "%d packets of the workload (all wavelengths) per step" % sample},
             "e2e": {"value": v, "unit": "packets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -172,11 +261,10 @@ def _has_gpu():
         return False
 
 
-def _density_for(model, tree):
+def _density_for(model):
     """Cell densities sampled on the device (DustSystem::setSampleDensityBody), read back so the
     CPU baseline uses the same ones."""
     from skirt7_b200 import runtime
-    model.dustGrid = tree
     model.rho = None
     ctx = runtime.Context(model, 0)
     rho = ctx.density()
@@ -184,16 +272,17 @@ def _density_for(model, tree):
     return rho
 
 
-def _config(args, tree):
-    return {"workload": "panchromatic octree disk galaxy: %d wavelengths 0.1-10 micron, octree max level %d, "
-                        "mass fraction %g (%d leaves), 3 frames 512x512 at 0/60/88 deg" %
-                        (args.nlambda, args.max_level, args.mass_fraction, tree.ncells if tree is not None else -1),
-            "packets_per_wavelength_per_gpu": args.packets, "nlambda": args.nlambda,
-            "cells": tree.ncells if tree is not None else None,
+def _config(args, wl):
+    return {"workload": wl.desc, "name": wl.name,
+            "packets_per_wavelength_per_gpu": args.packets, "nlambda": wl.model.wavelengthGrid.Nlambda,
+            "cells": wl.model.dustGrid.ncells, "grid_build_s": wl.grid_s,
             "geometry_precision": args.precision, "tallies": "fp64",
-            "l2": "working set (node records, neighbour lists, 315 MB of frames) exceeds the 126 MB L2",
+            "l2": "inputs larger than the 126 MB L2 (grid records, densities, frames); no flush between steps",
             "parallelism": "dp%d (packet ranges per GPU, NCCL all-reduce of frames per step)" % args.gpus}
 
+
+# ---------------------------------------------------------------------------------------------
+# the device arm
 
 def main():
     args = parse()
@@ -215,10 +304,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
-    model = build_model(args)
-    tree, tree_s = get_tree(args, model, local)
-    model.dustGrid = tree
-    model.rho = None
+    wl = Workload(args, local)
+    model = wl.model
     ctx = runtime.Context(model, device=local)
     nl = model.wavelengthGrid.Nlambda
     ells = np.arange(nl, dtype=np.int32)
@@ -229,21 +316,31 @@ def main():
     # a dedicated stream: the launches, the events and the collective all go on it
     tstream = torch.cuda.Stream(device=local)
     handle = tstream.cuda_stream
+    fr = wl.frames()
+    sizes = [_tally_len(ctx, i) for i in fr]
     # per-rank frames handed to the all-reduce (Instrument::sumResults, Instrument.cpp:57-65)
-    red = [torch.zeros(nl * 512 * 512, dtype=torch.float64, device="cuda") for _ in range(3)] if dist else None
+    red = [torch.zeros(n, dtype=torch.float64, device="cuda") for n in sizes] if dist else None
+    phases = [A.PHASE_STELLAR] + ([A.PHASE_DUST_EMISSION] if wl.dust_phase else [])
+
+    def run_phases(seed, stream):
+        ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=seed, precision=prec, stream=stream)
+        if wl.dust_phase:
+            ctx.calc_dust_emission()            # PanDustSystem::calculatedustemission
+            ctx.run_phase(A.PHASE_DUST_EMISSION, ells, Npp, first, npp_rank, seed=seed + 1, precision=prec,
+                          stream=stream)
 
     def step(seed):
-        ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=seed, precision=prec, stream=handle)
+        run_phases(seed, handle)
         if dist:
             with torch.cuda.stream(tstream):
-                for i, t in enumerate(red):
+                for i, t in zip(fr, red):
                     ctx.read_instrument_device(i, t.data_ptr(), None, handle)
                     dist.all_reduce(t)
 
     ctx.reset_tallies()
     ctx.sync()
     for w in range(args.warmup):
-        step(1000 + w)
+        step(1000 + 10 * w)
     torch.cuda.synchronize()
     ctx.counters()   # also checks the error word
 
@@ -256,7 +353,7 @@ def main():
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     for s in range(args.steps):
         ev[s][0].record(tstream)
-        step(2000 + s)
+        step(2000 + 10 * s)
         ev[s][1].record(tstream)
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -268,28 +365,24 @@ def main():
         total_ms = float(t.item())
         dist.barrier()
     torch.cuda.synchronize()
-    packets = Npp * nl * args.steps                # all ranks together
+    packets = Npp * nl * len(phases) * args.steps  # all ranks together
     value = packets / (total_ms / 1e3)
 
-    # kernel times and counters of one more step for the roofline: the traversal pass is the
-    # dominant kernel; its device time is summed over the waves of the phase (CUDA events around
-    # each launch on the launching stream)
+    # kernel times and counters of one more stellar phase for the roofline: the traversal pass is
+    # the dominant kernel; its device time is summed over the waves of the phase (CUDA events
+    # around each launch on the launching stream)
     ctx.reset_tallies()
     ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=999, precision=prec, stream=handle)
     ctx.sync()
     kms = ctx.last_phase_ms()
     ev_ms, trav_ms, waves = ctx.phase_times()
     c = ctx.counters()
-    # algorithmic bytes of the traversal pass (FP32 octree): per cell step the leaf box (24 B) and
-    # the cell density (4 B) of the current leaf; per followed rope its id (4 B); per absorption
-    # tally 8 B (the FP64 walk reads 48 B boxes and 8 B densities)
-    bstep = 4 + 24 if prec == A.PREC_FP32 else 8 + 48
-    alg_bytes = c["steps"] * bstep + c["nbr_scanned"] * 4 + 8 * c["absorb_adds"]
+    alg_bytes = wl.alg_bytes(c, prec == A.PREC_FP32)
     peak, peak_kind = peaks()
-    achieved = alg_bytes / waves / (trav_ms / waves / 1e3) / 1e9 if waves else 0.0
+    achieved = alg_bytes / (trav_ms / 1e3) / 1e9 if trav_ms > 0 else 0.0
 
-    # ---- end to end through the C ABI with host buffers: reset, run, read the 3 frames to host
-    cubes_bytes = sum(8 * nl * 512 * 512 for _ in range(3))
+    # ---- end to end through the C ABI with host buffers: reset, run, read the frames to host
+    cubes_bytes = 8 * sum(sizes)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -298,13 +391,13 @@ def main():
         ctx.reset_tallies()
         if dist:
             ctx.sync()
-            step(3000 + s)
+            step(3000 + 10 * s)
             if rank == 0:
                 host = [t.cpu() for t in red]      # the reduced frames, device -> host
             torch.cuda.synchronize()
         else:
-            ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=3000 + s, precision=prec)
-            for i in range(3):
+            run_phases(3000 + 10 * s, None)
+            for i in fr:
                 ctx.read_instrument(i)             # synchronises, then device -> host
     e2e_s = time.perf_counter() - t0
     if dist:
@@ -315,28 +408,29 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args, model, tree, ctx)
-    srv = serving_leg(args, local) if (rank == 0 and world == 1 and args.serving > 0) else None
+        cpu = cpu_baseline(args, wl, ctx)
+    srv = None
+    if rank == 0 and world == 1 and args.serving > 0 and args.workload == "octree_pan":
+        srv = serving_leg(args, local)
 
     if rank == 0:
         line = {
-            "metric": "photon packets/s (stellar emission, octree pan disk)",
+            "metric": wl.metric,
             "value": value, "unit": "packets/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if prec == A.PREC_FP32 else "f64", "data": "synthetic",
-            "config": _config(args, tree),
+            "config": _config(args, wl),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "trav_kernel (traversal pass)",
+                         "kernel": "trav_kernel (traversal pass of the stellar phase)",
                          "algorithmic_bytes_per_launch": alg_bytes / max(waves, 1),
-                         "kernel_ms_per_launch": trav_ms / max(waves, 1), "launches_per_step": waves,
+                         "kernel_ms_per_launch": trav_ms / max(waves, 1), "launches_per_phase": waves,
                          "phase_ms": kms, "event_pass_ms": ev_ms, "traversal_pass_ms": trav_ms},
-            "e2e": {"value": e2e, "unit": "packets/s", "h2d_bytes_per_step": 4 * nl + 64,
+            "e2e": {"value": e2e, "unit": "packets/s", "h2d_bytes_per_step": len(phases) * (4 * nl + 64),
                     "d2h_bytes_per_step": cubes_bytes},
-            "gpu_launches": 2 * waves * args.steps,
+            "gpu_launches": 2 * waves * len(phases) * args.steps,
             "clocks": clk,
-            "counters_last_step": c,
-            "tree_build_s": tree_s,
+            "counters_stellar_phase": c,
         }
         if cpu:
             line["cpu_baseline"] = cpu
@@ -348,11 +442,19 @@ def main():
         dist.destroy_process_group()
 
 
+def _tally_len(ctx, i):
+    import ctypes as C
+    cl, sl = C.c_int64(), C.c_int64()
+    ctx.lib.skg_tally_sizes(ctx.h, i, C.byref(cl), C.byref(sl))
+    return cl.value
+
+
 def serving_leg(args, device):
     """Fit-variant requests (oligochromatic disk, 3 wavelengths, Cartesian N^3 with N in 32..128,
     packets per wavelength log-uniform in 1e5..1e7, one 256x256 frame) arriving as a Poisson stream
     at 20/s, served by continuous batching; then every request alone on the idle device (the plain
     single-simulation path).  Latency = result in host memory minus arrival."""
+    import numpy as np
     from skirt7_b200 import serving
     reqs = serving.fitskirt_requests(n=args.serving, rate=20.0, seed=2024)
     srv = serving.Server(device=device, max_slots=64, tick_packets=1 << 19, npix=256)
@@ -361,12 +463,7 @@ def serving_leg(args, device):
     wall = time.perf_counter() - t0
     srv.close()
     st = serving.latency_stats(done)
-    alone = []
-    for r in reqs:
-        _, sec = serving.run_alone(r, device=device, npix=256)
-        alone.append(sec)
-    alone = sorted(alone)
-    import numpy as np
+    alone = sorted(serving.run_alone(r, device=device, npix=256)[1] for r in reqs)
     a50, a99 = float(np.percentile(alone, 50)), float(np.percentile(alone, 99))
     packets = sum(3 * r.packets for r in reqs)
     return {"requests": len(reqs), "arrival_rate_per_s": 20.0, "p50_s": st["p50_s"], "p99_s": st["p99_s"],
@@ -375,20 +472,22 @@ def serving_leg(args, device):
             "peak_resident": srv.peak_resident}
 
 
-def cpu_baseline(args, model, tree, ctx):
+def cpu_baseline(args, wl, ctx):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     oracle.build()
+    model = wl.model
     model.rho = ctx.density()
     threads = os.cpu_count() or 1
-    probe = oracle.simulate(model, args.packets, nthreads=threads, seed=1, max_packets=2000)
+    kw = dict(dust_emission_phase=wl.dust_phase)
+    probe = oracle.simulate(model, args.packets, nthreads=threads, seed=1, max_packets=2000, **kw)
     rate = probe["stats"]["packets"] / max(probe["stats"]["seconds"], 1e-6)
     sample = int(max(1000, min(2e6, rate * args.cpu_seconds)))
-    r = oracle.simulate(model, args.packets, nthreads=threads, seed=2, max_packets=sample)
+    r = oracle.simulate(model, args.packets, nthreads=threads, seed=2, max_packets=sample, **kw)
     model.rho = None
     return {"value": r["stats"]["packets"] / r["stats"]["seconds"], "unit": "packets/s", "cores": threads,
             "kind": "port", "sample": "%d packets over all %d wavelengths (%.1f s)" %
-                                      (r["stats"]["packets"], args.nlambda, r["stats"]["seconds"])}
+                                      (r["stats"]["packets"], model.wavelengthGrid.Nlambda, r["stats"]["seconds"])}
 
 
 if __name__ == "__main__":

@@ -237,6 +237,14 @@ DevGrid make_grid(Allocs& A, const skg_grid& g, cudaStream_t s) {
             }
         }
         G.vplane = upload(A, pl.data(), pl.size(), s);
+        // per entry the neighbour with its own entry range, so that the FP32 walk reaches the next
+        // cell's planes with one load
+        std::vector<int4> nx4((size_t)tot);
+        for (int64_t q = 0; q < tot; q++) {
+            int mi = g.vnbr_ids[q];
+            nx4[q] = (mi >= 0) ? make_int4(mi, off[mi], off[mi + 1], 0) : make_int4(mi, 0, 0, 0);
+        }
+        G.vnext = upload(A, nx4.data(), nx4.size(), s);
         G.nb = g.nb;
         size_t nb3 = (size_t)g.nb * g.nb * g.nb;
         int64_t btot = g.block_offsets[nb3];
@@ -507,6 +515,8 @@ int skg_ctx_create(const skg_scene* sc, int device, skg_ctx** out) {
             }
             ctx->sed_len[i] = (int64_t)I.ncomp * nl;
             I.sed = zeros<double>(A, ctx->sed_len[i], s);
+            H.sed_base[i] = H.sed_bins;
+            H.sed_bins += (int)ctx->sed_len[i];
         }
         // direction groups: instruments with the same observer direction share one peel-off traversal
         {

@@ -59,6 +59,7 @@ struct DevGrid {
     const int*    vnoff;
     const int*    vnbr;
     const float4* vplane;
+    const int4*   vnext;       // per CSR entry: (neighbour, its first entry, its end entry, 0)
     int nb;
     const int*    boff;
     const int*    bids;
@@ -603,6 +604,7 @@ template<typename R>
 struct VoronoiStepper {
     R x, y, z, kx, ky, kz;
     int mr;
+    int qb, qe;                 // neighbour entries of the current cell (FP32 walk; qe < 0: not read yet)
     Pend<R> pd;
     bool done;
     int steps;
@@ -615,7 +617,7 @@ struct VoronoiStepper {
     // segment); accepted for a position strictly inside the domain
     SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz, int hint = -1) {
         kx = dx; ky = dy; kz = dz; pd.clear(); done = false; steps = 0; fallbacks = 0; scanned = 0;
-        cell0 = -1;
+        cell0 = -1; qb = 0; qe = -1;
         if (hint >= 0 && rx > (R)g.xmin && rx < (R)g.xmax && ry > (R)g.ymin && ry < (R)g.ymax &&
             rz > (R)g.zmin && rz < (R)g.zmax) {
             mr = hint; cell0 = hint; x = rx; y = ry; z = rz;
@@ -690,11 +692,13 @@ SKG_D bool VoronoiStepper<double>::walk(const DevGrid& g, int& m, double& ds) {
 // FP32: precomputed bisector planes, one 16-byte load per neighbour entry
 template<>
 SKG_D bool VoronoiStepper<float>::walk(const DevGrid& g, int& m, float& ds) {
+    if (qe < 0 && !done) { qb = g.vnoff[mr]; qe = g.vnoff[mr + 1]; }
     while (!done) {
         if (++steps > g.max_steps) { done = true; return false; }
         float sq = FLT_MAX;
         int qbest = -1;
-        int q0 = g.vnoff[mr], q1 = g.vnoff[mr + 1];
+        const int q0 = qb, q1 = qe;
+#pragma unroll 4
         for (int q = q0; q < q1; q++) {
             float4 pl = __ldg(g.vplane + q);
             float ndotk = pl.x * kx + pl.y * ky + pl.z * kz;
@@ -709,11 +713,13 @@ SKG_D bool VoronoiStepper<float>::walk(const DevGrid& g, int& m, float& ds) {
             mr = voronoi_cell_index<float>(g, x, y, z);
             fallbacks++;
             if (mr < 0) done = true;
+            else { qb = g.vnoff[mr]; qe = g.vnoff[mr + 1]; }
             continue;
         }
         m = mr;
         x += (sq + g.epsf) * kx; y += (sq + g.epsf) * ky; z += (sq + g.epsf) * kz;
-        mr = __ldg(g.vnbr + qbest);
+        const int4 e = __ldg(g.vnext + qbest);
+        mr = e.x; qb = e.y; qe = e.z;
         if (mr < 0) done = true;
         ds = (mr >= 0) ? sq + g.epsf : sq;   // the nudge is credited to this segment (exact total length)
         return true;

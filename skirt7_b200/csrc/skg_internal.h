@@ -39,10 +39,6 @@ cudaError_t launch_emission_sources(const DevScene* dS, int nlambda, int ncells,
 size_t emission_scan_scratch_bytes(int ncells);
 cudaError_t launch_sum(const double* x, int64_t n, double* out, cudaStream_t s);
 cudaError_t launch_embed_density(const DevGrid& g, const float* rhof, cudaStream_t s);
-cudaError_t launch_voronoi_cells(const double* sites, int nsites, const double* ext, const int* gcell_off,
-                                 const int* gcell_ids, int gn, int kmax, int* nbr_count, int* nbr_ids,
-                                 double* volume, double* centroid, double* bbox, int* status,
-                                 cudaStream_t s);
 
 // skg_host.cpp
 void sersic_table(double n, double* sv, double* Sv, double* Mv);      // 101 points each

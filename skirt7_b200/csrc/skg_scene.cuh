@@ -63,6 +63,8 @@ struct DevScene {
     int group_instr[MAX_INSTR];
     int group_frame_only[MAX_INSTR];  // all members are Frame instruments (pixel test before traversal)
     double gkx[MAX_INSTR], gky[MAX_INSTR], gkz[MAX_INSTR];
+    int sed_base[MAX_INSTR];          // offset of each instrument's SED bins in a concatenation
+    int sed_bins;                     // SED bins of all instruments
 
     double min_weight_reduction;
     int min_scatt_events;

@@ -58,26 +58,34 @@ template<typename R> SKG_D double kappa_rho(const DevScene& S, int m, int ell) {
 
 // Instrument::detect for the members of one direction group after the shared traversal
 // (SEDInstrument.cpp:32-42, FrameInstrument.cpp:33-47, SimpleInstrument.cpp:35-49,
-// FullInstrument.cpp:109-177).  Returns the number of tally updates.
+// FullInstrument.cpp:109-177).  SED bins go to the block's private copy `psed` when it is given
+// (every packet of a wavelength adds to the same SED bin: global atomics would serialise on it).
+// Returns the number of tally updates.
 __device__ __noinline__ int detect_group(const DevScene& S, int grp, int ell, double Lpeel, double tau,
-                                         int nscatt_peel, bool stellar, double x, double y, double z) {
+                                         int nscatt_peel, bool stellar, double x, double y, double z, double* psed) {
     double Lextf = Lpeel * exp(-tau);
     const int nl = S.nlambda;
     int adds = 0;
     for (int q = S.group_start[grp]; q < S.group_start[grp + 1]; q++) {
-        const DevInstr& I = S.instr[S.group_instr[q]];
+        const int iq = S.group_instr[q];
+        const DevInstr& I = S.instr[iq];
+        auto sed_add = [&](int c, double v) {
+            if (psed) atomicAdd(psed + S.sed_base[iq] + c * nl + ell, v);
+            else atomicAdd(I.sed + (size_t)c * nl + ell, v);
+            adds++;
+        };
         int l = (I.type == SKG_INSTR_SED) ? -1 : pixel_on_detector(I, x, y, z);
         size_t fp = (size_t)I.nxp * I.nyp;
         if (I.type == SKG_INSTR_FRAME) {
             if (l >= 0) { atomicAdd(I.cube + (size_t)ell * fp + l, Lextf); adds++; }
         } else if (I.type == SKG_INSTR_SED) {
-            atomicAdd(I.sed + ell, Lextf); adds++;
+            sed_add(0, Lextf);
         } else if (I.type == SKG_INSTR_SIMPLE) {
-            atomicAdd(I.sed + ell, Lextf); adds++;
+            sed_add(0, Lextf);
             if (l >= 0) { atomicAdd(I.cube + (size_t)ell * fp + l, Lextf); adds++; }
         } else {
             auto add = [&](int c, double v) {
-                atomicAdd(I.sed + (size_t)c * nl + ell, v); adds++;
+                sed_add(c, v);
                 if (l >= 0) { atomicAdd(I.cube + ((size_t)c * nl + ell) * fp + l, v); adds++; }
             };
             add(SKG_FULL_TOT, Lextf);
@@ -254,13 +262,20 @@ SKG_D int peel_jobs(const DevScene& S, int ell, bool scat, int cell, double kx, 
     return n;
 }
 
+constexpr int SED_PRIV = 1024;          // SED bins a block keeps privately (8 KB)
+
 template<typename R>
 __global__ void __launch_bounds__(256) event_kernel(const WaveParams W) {
     __shared__ unsigned long long s_cnt[C_N];
-    if (threadIdx.x < C_N) s_cnt[threadIdx.x] = 0;
-    __syncthreads();
+    __shared__ double s_sed[SED_PRIV];
     const RunParams& P = W.R;
     const BatchHeader H = *P.hdr;
+    // a launch of one simulation tallies its SED bins per block and adds them once at the end
+    const int sed_bins = (H.nslots == 1) ? P.scenes[0]->sed_bins : 0;
+    double* const psed = (sed_bins > 0 && sed_bins <= SED_PRIV) ? s_sed : nullptr;
+    if (threadIdx.x < C_N) s_cnt[threadIdx.x] = 0;
+    if (psed) for (int t = threadIdx.x; t < sed_bins; t += blockDim.x) s_sed[t] = 0.0;
+    __syncthreads();
     const int phase = H.phase;
     const bool peel_on = phase != SKG_PHASE_DUST_SELFABS;
     const int lane = threadIdx.x & 31;
@@ -282,7 +297,8 @@ __global__ void __launch_bounds__(256) event_kernel(const WaveParams W) {
         int pix = 0;
         for (int i = 0; i < K.peel_n; i++) {
             const int j = K.peel_j0 + i;
-            pix += detect_group(S, W.pjobs[j].y, K.ell, W.pjL[j], W.pjtau[j], nsp, (K.flags & 1) != 0, K.x, K.y, K.z);
+            pix += detect_group(S, W.pjobs[j].y, K.ell, W.pjL[j], W.pjtau[j], nsp, (K.flags & 1) != 0, K.x, K.y, K.z,
+                                psed);
         }
         atomicAdd(&s_cnt[C_PIX], (unsigned long long)pix);
         atomicAdd(&s_cnt[C_PEEL], (unsigned long long)K.peel_n);
@@ -398,6 +414,16 @@ __global__ void __launch_bounds__(256) event_kernel(const WaveParams W) {
     }
     __syncthreads();
     if (threadIdx.x < C_N && s_cnt[threadIdx.x]) atomicAdd(P.counters + threadIdx.x, s_cnt[threadIdx.x]);
+    if (psed) {
+        const DevScene& S0 = *P.scenes[0];
+        for (int t = threadIdx.x; t < sed_bins; t += blockDim.x) {
+            const double v = s_sed[t];
+            if (v == 0.0) continue;
+            int i = 0;
+            while (i + 1 < S0.ninstr && S0.sed_base[i + 1] <= t) i++;
+            atomicAdd(S0.instr[i].sed + (t - S0.sed_base[i]), v);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -18,16 +18,21 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <type_traits>
 #include <vector>
 
 using namespace skg;
 
 namespace {
 
+// capacities of the device construction (a cell that exceeds one is rebuilt on the host with
+// the larger ones below)
 constexpr int VMAXP = 112;     // clipping planes per cell (6 walls included)
 constexpr int VMAXT = 224;     // dual triangles (polyhedron vertices)
 constexpr int VMAXC = 96;      // candidates per shell
 constexpr int VMAXN = 80;      // neighbours stored per cell
+constexpr int HMAXP = 1024, HMAXT = 2048, HMAXC = 512, HMAXN = 1000;
 
 struct BinGrid {
     double lo[3], h[3];
@@ -38,7 +43,8 @@ struct BinGrid {
 
 struct Plane { double x, y, z, d; };
 
-__host__ __device__ __forceinline__ void tri_vertex(const Plane* P, const unsigned char* t, double* v) {
+template<typename I>
+__host__ __device__ __forceinline__ void tri_vertex(const Plane* P, const I* t, double* v) {
     const Plane &a = P[t[0]], &b = P[t[1]], &c = P[t[2]];
     // Cramer: v = (d_a (b x c) + d_b (c x a) + d_c (a x b)) / (a . (b x c))
     double bcx = b.y * c.z - b.z * c.y, bcy = b.z * c.x - b.x * c.z, bcz = b.x * c.y - b.y * c.x;
@@ -51,16 +57,20 @@ __host__ __device__ __forceinline__ void tri_vertex(const Plane* P, const unsign
     v[2] = (a.d * bcz + b.d * caz + c.d * abz) * inv;
 }
 
-// Builds cell i; host-callable as well so that the clipping can be checked without a device.
-__host__ __device__ void voronoi_cell(int i, const double* __restrict__ sites, const double* __restrict__ ext,
-                                      const BinGrid& G, int* nbr_count, int* nbr_ids, double* volume,
-                                      double* centroid, double* bbox, int* status) {
+// Builds the cell of site i with capacities MP planes, MT polyhedron vertices, MC candidates per
+// batch and MN stored neighbours, writing its results to output slot o; callable on the host too
+// (the rebuild of cells that exceed the device capacities).
+template<int MP, int MT, int MC, int MN>
+__host__ __device__ void voronoi_cell_t(int i, int o, const double* __restrict__ sites, const double* __restrict__ ext,
+                                        const BinGrid& G, int* nbr_count, int* nbr_ids, double* volume,
+                                        double* centroid, double* bbox, int* status) {
+    using PIdx = typename std::conditional<(MP <= 255), unsigned char, unsigned short>::type;
     const double px = sites[3 * i], py = sites[3 * i + 1], pz = sites[3 * i + 2];
 
-    Plane P[VMAXP];
-    int pid[VMAXP];
-    unsigned char T[VMAXT][3];
-    double V[VMAXT][3];
+    Plane P[MP];
+    int pid[MP];
+    PIdx T[MT][3];
+    double V[MT][3];
     int np = 6, nt = 0;
     int st = 0;
 
@@ -72,7 +82,7 @@ __host__ __device__ void voronoi_cell(int i, const double* __restrict__ sites, c
     P[4] = {0, 0, -1, -(ext[2] - pz)}; pid[4] = -5;
     P[5] = {0, 0, 1, ext[5] - pz};     pid[5] = -6;
     for (int c = 0; c < 8; c++) {
-        unsigned char a = (c & 1) ? 1 : 0, b = (c & 2) ? 3 : 2, d = (c & 4) ? 5 : 4;
+        PIdx a = (c & 1) ? 1 : 0, b = (c & 2) ? 3 : 2, d = (c & 4) ? 5 : 4;
         // orientation: det(n_a, n_b, n_d) > 0
         double s = P[a].x * (P[b].y * P[d].z - P[b].z * P[d].y) - P[a].y * (P[b].x * P[d].z - P[b].z * P[d].x)
                  + P[a].z * (P[b].x * P[d].y - P[b].y * P[d].x);
@@ -88,9 +98,9 @@ __host__ __device__ void voronoi_cell(int i, const double* __restrict__ sites, c
     int b1 = max(0, min(G.n[1] - 1, (int)((py - G.lo[1]) / G.h[1])));
     int b2 = max(0, min(G.n[2] - 1, (int)((pz - G.lo[2]) / G.h[2])));
     int maxs = max(G.n[0], max(G.n[1], G.n[2]));
-    int cand[VMAXC];
-    double cd2[VMAXC];
-    bool outside[VMAXT];
+    int cand[MC];
+    double cd2[MC];
+    bool outside[MT];
 
     for (int s = 0; s <= maxs && !st; s++) {
         // smallest distance from the site to any bin at Chebyshev distance >= s
@@ -137,7 +147,7 @@ __host__ __device__ void voronoi_cell(int i, const double* __restrict__ sites, c
             int k = nc++;
             while (k > 0 && cd2[k - 1] > d2next) { cd2[k] = cd2[k - 1]; cand[k] = cand[k - 1]; k--; }
             cd2[k] = d2next; cand[k] = jnext;
-            if (nc < VMAXC) continue;
+            if (nc < MC) continue;
           }
           // clip by the collected candidates, nearest first
           for (int c = 0; c < nc && !st; c++) {
@@ -151,27 +161,27 @@ __host__ __device__ void voronoi_cell(int i, const double* __restrict__ sites, c
                 nout += outside[t];
             }
             if (nout == 0) continue;
-            if (nout == nt || np >= VMAXP) { st = 2; break; }
+            if (nout == nt || np >= MP) { st = 2; break; }
             int pnew = np;
             P[np] = {nx, ny, nz, d}; pid[np] = j; np++;
             // new triangles on the boundary of the removed region
             int nnew = 0;
-            unsigned char NT[VMAXT][3];
+            PIdx NT[MT][3];
             for (int t = 0; t < nt && !st; t++) {
                 if (!outside[t]) continue;
                 for (int e = 0; e < 3; e++) {
-                    unsigned char x = T[t][e], y = T[t][(e + 1) % 3];
+                    PIdx x = T[t][e], y = T[t][(e + 1) % 3];
                     // the triangle across edge x->y holds y->x
                     int u = -1;
                     for (int w = 0; w < nt; w++) {
                         if (w == t) continue;
-                        const unsigned char* W = T[w];
+                        const PIdx* W = T[w];
                         if ((W[0] == y && W[1] == x) || (W[1] == y && W[2] == x) || (W[2] == y && W[0] == x)) { u = w; break; }
                     }
                     if (u < 0) { st = 3; break; }
                     if (!outside[u]) {
-                        if (nnew >= VMAXT) { st = 1; break; }
-                        NT[nnew][0] = x; NT[nnew][1] = y; NT[nnew][2] = (unsigned char)pnew; nnew++;
+                        if (nnew >= MT) { st = 1; break; }
+                        NT[nnew][0] = x; NT[nnew][1] = y; NT[nnew][2] = (PIdx)pnew; nnew++;
                     }
                 }
             }
@@ -183,7 +193,7 @@ __host__ __device__ void voronoi_cell(int i, const double* __restrict__ sites, c
                               V[w][0] = V[t][0]; V[w][1] = V[t][1]; V[w][2] = V[t][2]; }
                 w++;
             }
-            if (w + nnew > VMAXT) { st = 1; break; }
+            if (w + nnew > MT) { st = 1; break; }
             for (int q = 0; q < nnew; q++) {
                 T[w][0] = NT[q][0]; T[w][1] = NT[q][1]; T[w][2] = NT[q][2];
                 tri_vertex(P, T[w], V[w]);
@@ -209,14 +219,14 @@ __host__ __device__ void voronoi_cell(int i, const double* __restrict__ sites, c
         for (int t = 0; t < nt && t0 < 0; t++)
             for (int c = 0; c < 3; c++) if (T[t][c] == p) { t0 = t; k0 = c; break; }
         if (t0 < 0) continue;
-        if (nn >= VMAXN) { st = 1; break; }
-        nbr_ids[(size_t)i * VMAXN + nn++] = pid[p];
+        if (nn >= MN) { st = 1; break; }
+        nbr_ids[(size_t)o * MN + nn++] = pid[p];
         // walk around plane p: triangle (p, a, b) -> the triangle holding p followed by b
         int t = t0, k = k0, guard = 0;
         const double* A0 = V[t0];
         const double* prev = nullptr;
         do {
-            unsigned char b = T[t][(k + 2) % 3];
+            PIdx b = T[t][(k + 2) % 3];
             const double* cur = V[t];
             if (prev) {
                 // tetrahedron (site, A0, prev, cur)
@@ -231,17 +241,17 @@ __host__ __device__ void voronoi_cell(int i, const double* __restrict__ sites, c
                 for (int c = 0; c < 3; c++) if (T[w][c] == p && T[w][(c + 1) % 3] == b) { nxt = w; nk = c; break; }
             if (nxt < 0) { st = 3; break; }
             t = nxt; k = nk;
-        } while (t != t0 && ++guard < VMAXT);
-        if (guard >= VMAXT) st = 3;
+        } while (t != t0 && ++guard < MT);
+        if (guard >= MT) st = 3;
     }
-    nbr_count[i] = nn;
+    nbr_count[o] = nn;
     double V6 = vol;
-    volume[i] = fabs(V6) / 6.0;
-    if (V6 != 0) { centroid[3 * i] = px + cx / (4.0 * V6); centroid[3 * i + 1] = py + cy / (4.0 * V6); centroid[3 * i + 2] = pz + cz / (4.0 * V6); }
-    else { centroid[3 * i] = px; centroid[3 * i + 1] = py; centroid[3 * i + 2] = pz; }
-    bbox[6 * i] = px + lo[0]; bbox[6 * i + 1] = py + lo[1]; bbox[6 * i + 2] = pz + lo[2];
-    bbox[6 * i + 3] = px + hi[0]; bbox[6 * i + 4] = py + hi[1]; bbox[6 * i + 5] = pz + hi[2];
-    status[i] = st;
+    volume[o] = fabs(V6) / 6.0;
+    if (V6 != 0) { centroid[3 * o] = px + cx / (4.0 * V6); centroid[3 * o + 1] = py + cy / (4.0 * V6); centroid[3 * o + 2] = pz + cz / (4.0 * V6); }
+    else { centroid[3 * o] = px; centroid[3 * o + 1] = py; centroid[3 * o + 2] = pz; }
+    bbox[6 * o] = px + lo[0]; bbox[6 * o + 1] = py + lo[1]; bbox[6 * o + 2] = pz + lo[2];
+    bbox[6 * o + 3] = px + hi[0]; bbox[6 * o + 4] = py + hi[1]; bbox[6 * o + 5] = pz + hi[2];
+    status[o] = st;
 }
 
 __global__ void voronoi_cell_kernel(const double* __restrict__ sites, int nsites, const double* __restrict__ ext,
@@ -249,7 +259,7 @@ __global__ void voronoi_cell_kernel(const double* __restrict__ sites, int nsites
                                     double* bbox, int* status) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nsites) return;
-    voronoi_cell(i, sites, ext, G, nbr_count, nbr_ids, volume, centroid, bbox, status);
+    voronoi_cell_t<VMAXP, VMAXT, VMAXC, VMAXN>(i, i, sites, ext, G, nbr_count, nbr_ids, volume, centroid, bbox, status);
 }
 
 }  // namespace
@@ -350,13 +360,37 @@ int skg_voronoi_build(const double* sites, int32_t nsites, double xmin, double y
             cudaMemcpy(v->centroid.data(), d[7], sz[7], cudaMemcpyDeviceToHost);
             cudaMemcpy(v->bbox.data(), d[8], sz[8], cudaMemcpyDeviceToHost);
             cudaMemcpy(status.data(), d[9], sz[9], cudaMemcpyDeviceToHost);
+            // cells beyond the device capacities (many neighbours, e.g. a sparse cell against a
+            // dense region) are rebuilt on the host with larger ones
+            BinGrid H;
+            for (int c = 0; c < 3; c++) { H.lo[c] = ext[c]; H.h[c] = gh[c]; H.n[c] = gn[c]; }
+            H.off = boff.data(); H.ids = bid.data();
+            std::map<int, std::vector<int>> big;
             int bad = 0;
-            for (int m = 0; m < n; m++) if (status[m]) bad++;
+            for (int m = 0; m < n; m++) {
+                if (!status[m]) continue;
+                int hc = 0, hst = 0;
+                std::vector<int> hid(HMAXN);
+                double hv, hcen[3], hbb[6];
+                voronoi_cell_t<HMAXP, HMAXT, HMAXC, HMAXN>(m, 0, v->sites.data(), ext, H, &hc, hid.data(), &hv, hcen,
+                                                           hbb, &hst);
+                if (hst) { bad++; continue; }
+                hid.resize(hc);
+                big[m] = hid;
+                cnt[m] = hc;
+                v->volume[m] = hv;
+                std::copy(hcen, hcen + 3, &v->centroid[3 * (size_t)m]);
+                std::copy(hbb, hbb + 6, &v->bbox[6 * (size_t)m]);
+            }
             if (bad) { rc = SKG_ERR_INVALID; err = "Voronoi cell construction failed for " + std::to_string(bad) + " cells"; }
             v->noff.assign(n + 1, 0);
             for (int m = 0; m < n; m++) v->noff[m + 1] = v->noff[m] + cnt[m];
             v->nbr.resize(v->noff[n]);
-            for (int m = 0; m < n; m++) std::copy(&ids[(size_t)m * VMAXN], &ids[(size_t)m * VMAXN] + cnt[m], &v->nbr[v->noff[m]]);
+            for (int m = 0; m < n; m++) {
+                auto it = big.find(m);
+                if (it != big.end()) std::copy(it->second.begin(), it->second.end(), &v->nbr[v->noff[m]]);
+                else std::copy(&ids[(size_t)m * VMAXN], &ids[(size_t)m * VMAXN] + cnt[m], &v->nbr[v->noff[m]]);
+            }
         }
         for (int q = 0; q < 10; q++) if (d[q]) cudaFree(d[q]);
     }
