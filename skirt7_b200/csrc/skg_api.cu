@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -182,8 +183,16 @@ DevGrid make_grid(Allocs& A, const skg_grid& g, cudaStream_t s) {
         // rope-linked tree for the FP32 walk
         {
             RopeTree rt;
-            build_rope_tree(g, rt);
-            G.lrec = upload(A, rt.lrec.data(), rt.lrec.size(), s);
+            // SKG_TREE_RECORDS=rope keeps the 64-byte leaf records for trees that fit the lattice
+            const char* rec = std::getenv("SKG_TREE_RECORDS");
+            build_rope_tree(g, rt, !(rec && std::strcmp(rec, "rope") == 0));
+            if (rt.lattice) {
+                G.prec = upload(A, rt.prec.data(), rt.prec.size(), s);
+                G.lattice = 1;
+                for (int a = 0; a < 3; a++) { G.lorg[a] = rt.lorg[a]; G.lunit[a] = rt.lunit[a]; }
+            } else {
+                G.lrec = upload(A, rt.lrec.data(), rt.lrec.size(), s);
+            }
             G.irec = upload(A, rt.irec.data(), std::max<size_t>(rt.irec.size(), 1), s);
             G.cell_leaf = upload(A, rt.cell_leaf.data(), rt.cell_leaf.size(), s);
             G.root_ref = rt.root_ref;
@@ -459,7 +468,7 @@ int skg_ctx_create(const skg_scene* sc, int device, skg_ctx** out) {
                 CK(cudaStreamSynchronize(s));
             }
             H.rhof = rf;
-            if (sc->ncomp == 1 && ctx->grid.lrec) CK(launch_embed_density(ctx->grid, rf, s));
+            if (sc->ncomp == 1 && (ctx->grid.lrec || ctx->grid.prec)) CK(launch_embed_density(ctx->grid, rf, s));
         }
 
         // stellar system (StellarSystem.cpp:35-52)
@@ -749,7 +758,7 @@ int skg_run_phase(skg_ctx* ctx, int phase, const int32_t* ells, int nell, uint64
         int precision = opts ? opts->precision : SKG_PREC_FP32;
         int blocks = opts ? opts->blocks : 0;
         CK(cudaEventRecord(ctx->ev0, s));
-        CK(ctx->waves.begin(P, ctx->grid.type, ctx->grid.search == SKG_SEARCH_BOOKKEEPING, precision, 1, npool, blocks, s));
+        CK(ctx->waves.begin(P, ctx->grid.type, tree_walk_of(ctx->grid), precision, 1, npool, blocks, s));
         CK(cudaEventRecord(ctx->ev1, s));
         return SKG_OK;
     } catch (const Failure& f) { return fail(ctx, f); }
@@ -1152,9 +1161,9 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
             auto tree = [](int t) { return t == SKG_GRID_OCTREE || t == SKG_GRID_BINTREE; };
             REQUIRE(w.ctx->grid.type == gtype || (tree(gtype) && tree(w.ctx->grid.type)),
                     "a batch holds one kind of grid");
-            const int bk = tree(gtype) && w.ctx->grid.search == SKG_SEARCH_BOOKKEEPING;
+            const int bk = tree(gtype) ? tree_walk_of(w.ctx->grid) : TW_ROPE;
             if (gbk < 0) gbk = bk;
-            REQUIRE(bk == gbk, "a batch holds trees of one search method kind (Bookkeeping or not)");
+            REQUIRE(bk == gbk, "a batch holds trees of one walk kind (Bookkeeping search, rope or lattice records)");
             if (phase != SKG_PHASE_STELLAR) REQUIRE(w.ctx->emit_cdf != nullptr, "dust phases need dust emission enabled");
             int slot = -1;
             for (int q = 0; q < nslots; q++) if (slots[q] == w.ctx) slot = q;
@@ -1204,7 +1213,7 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
             CK(cudaMemsetAsync(T.work, 0, sizeof(unsigned long long), q));
             CK(cudaMemsetAsync(T.err, 0, sizeof(unsigned), q));
             // every slot's DevGrid is copied into shared memory: size for the batch's capacity
-            CK(b->waves.begin(P, gtype < 0 ? SKG_GRID_CARTESIAN : gtype, gbk == 1, precision, T.max_slots, npool,
+            CK(b->waves.begin(P, gtype < 0 ? SKG_GRID_CARTESIAN : gtype, gbk < 0 ? TW_ROPE : gbk, precision, T.max_slots, npool,
                               blocks, q));
         };
         CK(cudaEventRecord(b->ev0, s));

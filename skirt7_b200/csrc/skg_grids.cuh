@@ -49,6 +49,11 @@ struct DevGrid {
     const float4* irec;
     const int*    cell_leaf;    // cell number -> leaf index
     int root_ref;
+    // lattice form (trees split at midpoints): 32-byte leaf records in cell order, walls at
+    // fmaf(integer, lunit, lorg); irec as above (layout: RopeTree in skg_tree.h)
+    const uint4*  prec;
+    int lattice;
+    float lorg[3], lunit[3];
 
     // Voronoi: sites (3 doubles / float4), CSR neighbours, FP32 bisector planes per CSR entry
     // vplane[q] = (n.x, n.y, n.z, n.p) with n = p_i - p_r and p the bisector midpoint; walls are
@@ -66,6 +71,13 @@ struct DevGrid {
     const double* vbbox;
     const double* vvol;        // Voronoi cell volumes
 };
+
+// The FP32 walk a tree grid takes: the node walk (Bookkeeping search), the 64-byte rope records or
+// their lattice form.
+enum TreeWalk : int { TW_ROPE = 0, TW_NODES = 1, TW_LATTICE = 2 };
+inline int tree_walk_of(const DevGrid& g) {
+    return g.search == SKG_SEARCH_BOOKKEEPING ? TW_NODES : g.lattice ? TW_LATTICE : TW_ROPE;
+}
 
 // ---------------------------------------------------------------------------------------------
 // precision traits
@@ -150,17 +162,18 @@ SKG_D bool move_inside(const DevGrid& g, R eps, R& rx, R& ry, R& rz, R kx, R ky,
 }
 
 // =============================================================================================
-// Cartesian
+// Cartesian: the reference's arithmetic (FP64, and the entry of the FP32 walk)
 template<typename R>
-struct CartStepper {
+struct CartStepperRef {
     R x, y, z, kx, ky, kz;
     int i, j, k;
     Pend<R> pd;
     bool done;
     int steps;
     int cell0;                  // cell holding the start position (-1 if it lies outside the grid)
-    static constexpr int scanned = 0, fallbacks = 0;
+    static constexpr int fallbacks = 0;
     static constexpr float rho = -1.f;   // density not embedded: the tracer reads it by cell
+    SKG_D int nscanned() const { return 0; }
 
     // hint: a cell known to hold the start position (or -1); it is verified against the planes
     SKG_D void init(const DevGrid& g, R rx, R ry, R rz, R dx, R dy, R dz, int hint = -1) {
@@ -251,6 +264,64 @@ struct CartStepper {
     }
 };
 
+template<typename R> struct CartStepper : CartStepperRef<R> {};
+
+// FP32 production walk of the Cartesian grid: after the reference's entry (nudge and cell
+// location), a DDA over the ray parameter t measured from the entry point.  The next wall of each
+// axis sits at t = (plane - origin) / k, computed once per crossing with a reciprocal taken once per
+// traversal; a segment is the difference of consecutive wall parameters (exact: Sterbenz), so no
+// position is updated and nothing accumulates along the path.  Ties resolve in the reference's
+// order x, y, z.
+template<>
+struct CartStepper<float> : CartStepperRef<float> {
+    float tx, ty, tz;           // ray parameter of the next x, y and z wall
+    float tc;                   // ray parameter of the current point
+    float ux, uy, uz;           // 1/k (unused for an axis with |k| <= 1e-15: never crossed)
+
+    SKG_D void init(const DevGrid& g, float rx, float ry, float rz, float dx, float dy, float dz, int hint = -1) {
+        CartStepperRef<float>::init(g, rx, ry, rz, dx, dy, dz, hint);
+        tc = 0.f;
+        if (done) return;
+        if (isnan(kx) || isnan(ky) || isnan(kz)) { done = true; return; }   // the reference walk stops
+        const bool mx = fabsf(kx) > 1e-15f, my = fabsf(ky) > 1e-15f, mz = fabsf(kz) > 1e-15f;
+        ux = mx ? 1.f / kx : 0.f; uy = my ? 1.f / ky : 0.f; uz = mz ? 1.f / kz : 0.f;
+        tx = mx ? (gx<float>(g, kx < 0.f ? i : i + 1) - x) * ux : FLT_MAX;
+        ty = my ? (gy<float>(g, ky < 0.f ? j : j + 1) - y) * uy : FLT_MAX;
+        tz = mz ? (gz<float>(g, kz < 0.f ? k : k + 1) - z) * uz : FLT_MAX;
+    }
+    SKG_D bool next(const DevGrid& g, int& m, float& ds) {
+        if (pd.pop(ds)) { m = -1; return true; }
+        return walk(g, m, ds);
+    }
+    SKG_D bool walk(const DevGrid& g, int& m, float& ds) {
+        while (!done) {
+            if (++steps > g.max_steps) { done = true; return false; }
+            m = k + g.nz * j + g.nz * g.ny * i;
+            float t;
+            if (tx <= ty && tx <= tz) {
+                t = tx;
+                i += (kx < 0.f) ? -1 : 1;
+                if (i >= g.nx || i < 0) done = true;
+                else tx = (gx<float>(g, kx < 0.f ? i : i + 1) - x) * ux;
+            } else if (ty < tx && ty <= tz) {
+                t = ty;
+                j += (ky < 0.f) ? -1 : 1;
+                if (j >= g.ny || j < 0) done = true;
+                else ty = (gy<float>(g, ky < 0.f ? j : j + 1) - y) * uy;
+            } else if (tz < tx && tz < ty) {
+                t = tz;
+                k += (kz < 0.f) ? -1 : 1;
+                if (k >= g.nz || k < 0) done = true;
+                else tz = (gz<float>(g, kz < 0.f ? k : k + 1) - z) * uz;
+            } else { done = true; return false; }   // NaN direction
+            const float d = t - tc;
+            tc = t;
+            if (d > 0.f) { ds = d; return true; }   // DustGridPath::addSegment drops ds <= 0
+        }
+        return false;
+    }
+};
+
 // =============================================================================================
 // Tree (octree and k-d tree)
 template<typename R> SKG_D void node_bounds(const DevGrid& g, int l, V3<R>& lo, V3<R>& hi);
@@ -304,6 +375,7 @@ struct TreeNodeWalk {
     int steps;
     int fallbacks;
     int scanned;
+    SKG_D int nscanned() const { return scanned; }
     int cell0;
     static constexpr float rho = -1.f;
 
@@ -461,7 +533,8 @@ struct TreeStepper<float> {
     int leaf;
     Pend<float> pd;
     bool done;
-    int steps, fallbacks, scanned;
+    int steps, fallbacks;
+    SKG_D int nscanned() const { return steps; }   // one rope followed per step
     int cell0;
     float rho;                  // density embedded in the record of the last segment's cell
 
@@ -496,7 +569,7 @@ struct TreeStepper<float> {
     }
 
     SKG_D void init(const DevGrid& g, float rx, float ry, float rz, float dx, float dy, float dz, int hint = -1) {
-        kx = dx; ky = dy; kz = dz; pd.clear(); done = false; steps = 0; fallbacks = 0; scanned = 0;
+        kx = dx; ky = dy; kz = dz; pd.clear(); done = false; steps = 0; fallbacks = 0;
         cell0 = -1; rho = -1.f;
         if (hint >= 0) {
             leaf = __ldg(g.cell_leaf + hint);
@@ -538,7 +611,6 @@ struct TreeStepper<float> {
             // follow the rope of the exit wall; if the point is not in the leaf it leads to (it
             // crossed near an edge or corner), locate it from the root
             int next = (rope == -1) ? -1 : descend(g, rope, x, y, z);
-            scanned++;
             if (next >= 0) {
                 load(g, next);
                 if (!inside(x, y, z)) {
@@ -559,6 +631,117 @@ struct TreeStepper<float> {
             }
             if (next < 0) done = true;
             else { leaf = next; d += eps; }      // the nudge is credited to the segment left behind
+            if (d > 0.f) { ds = d; return true; }
+        }
+        return false;
+    }
+};
+
+// FP32 walk on the lattice form of the rope tree: the same steps as TreeStepper<float>, with the
+// current leaf's 32-byte record (density, centre codes, packed ropes) in registers and its walls
+// computed from the codes.  A leaf reference is the cell number.
+template<typename R> struct TreeLatticeStepper : TreeNodeWalk<R> {};
+
+template<>
+struct TreeLatticeStepper<float> {
+    float x, y, z, kx, ky, kz;
+    uint4 a, b;                 // the current leaf's record
+    int leaf;                   // its cell number
+    Pend<float> pd;
+    bool done;
+    int steps, fallbacks;
+    SKG_D int nscanned() const { return steps; }   // one rope followed per step
+    int cell0;
+    float rho;
+
+    SKG_D void load(const DevGrid& g, int li) {
+        const uint4* p = g.prec + 2 * (size_t)li;
+        a = __ldg(p); b = __ldg(p + 1);
+    }
+    SKG_D static uint32_t code_x(const uint4& a) { return a.y & 0x1FFFFFu; }
+    SKG_D static uint32_t code_y(const uint4& a) { return __funnelshift_r(a.y, a.z, 21) & 0x1FFFFFu; }
+    SKG_D static uint32_t code_z(const uint4& a) { return (a.z >> 10) & 0x1FFFFFu; }
+    // the low (up = false) or high wall of the interval with centre code c
+    SKG_D static float wall(uint32_t c, bool up, float org, float unit) {
+        const uint32_t t = c & (0u - c);          // half the width: the code's lowest set bit
+        return fmaf((float)(up ? c + t : c - t), unit, org);
+    }
+    SKG_D static bool within(uint32_t c, float p, float org, float unit) {
+        const uint32_t t = c & (0u - c);
+        return p >= fmaf((float)(c - t), unit, org) && p <= fmaf((float)(c + t), unit, org);
+    }
+    SKG_D bool inside(const DevGrid& g, float px, float py, float pz) const {
+        return within(code_x(a), px, g.lorg[0], g.lunit[0]) && within(code_y(a), py, g.lorg[1], g.lunit[1]) &&
+               within(code_z(a), pz, g.lorg[2], g.lunit[2]);
+    }
+    // the reference of wall f: 26 bits at bit 26 f of the 160-bit string (a.w, b.x, b.y, b.z, b.w)
+    SKG_D int rope(int f) const {
+        const int bit = 26 * f, wd = bit >> 5, sh = bit & 31;
+        const uint32_t lo = wd == 0 ? a.w : wd == 1 ? b.x : wd == 2 ? b.y : wd == 3 ? b.z : b.w;
+        const uint32_t hi = wd == 0 ? b.x : wd == 1 ? b.y : wd == 2 ? b.z : b.w;
+        const uint32_t v = __funnelshift_r(lo, hi, sh) & 0x3FFFFFFu;
+        return v == 0x3FFFFFFu ? -1 : (v >= (1u << 25)) ? -(int)(v - (1u << 25)) - 2 : (int)v;
+    }
+
+    SKG_D void init(const DevGrid& g, float rx, float ry, float rz, float dx, float dy, float dz, int hint = -1) {
+        kx = dx; ky = dy; kz = dz; pd.clear(); done = false; steps = 0; fallbacks = 0;
+        cell0 = -1; rho = -1.f;
+        if (hint >= 0) {
+            leaf = hint;
+            load(g, leaf);
+            if (inside(g, rx, ry, rz)) { cell0 = hint; x = rx; y = ry; z = rz; return; }
+        }
+        bool ok = move_inside<float>(g, g.epsf, rx, ry, rz, kx, ky, kz, pd);
+        leaf = ok ? TreeStepper<float>::locate(g, rx, ry, rz) : -1;
+        if (leaf < 0) { pd.n = 0; done = true; return; }
+        load(g, leaf);
+        if (pd.n == 0) cell0 = leaf;
+        x = rx; y = ry; z = rz;
+    }
+
+    SKG_D bool next(const DevGrid& g, int& m, float& ds) {
+        if (pd.pop(ds)) { m = -1; rho = 0.f; return true; }
+        return walk(g, m, ds);
+    }
+    SKG_D bool walk(const DevGrid& g, int& m, float& ds) {
+        const float eps = g.epsf;
+        while (!done) {
+            if (++steps > g.max_steps) { done = true; return false; }
+            const float xnext = wall(code_x(a), kx >= 0.f, g.lorg[0], g.lunit[0]);
+            const float ynext = wall(code_y(a), ky >= 0.f, g.lorg[1], g.lunit[1]);
+            const float znext = wall(code_z(a), kz >= 0.f, g.lorg[2], g.lunit[2]);
+            float dsx = (fabsf(kx) > 1e-15f) ? (xnext - x) / kx : FLT_MAX;
+            float dsy = (fabsf(ky) > 1e-15f) ? (ynext - y) / ky : FLT_MAX;
+            float dsz = (fabsf(kz) > 1e-15f) ? (znext - z) / kz : FLT_MAX;
+            float d; int face;          // exit wall: 0..5 = x-, x+, y-, y+, z-, z+
+            if (dsx <= dsy && dsx <= dsz) { d = dsx; face = (kx < 0.f) ? 0 : 1; }
+            else if (dsy <= dsx && dsy <= dsz) { d = dsy; face = (ky < 0.f) ? 2 : 3; }
+            else { d = dsz; face = (kz < 0.f) ? 4 : 5; }
+            const int rp = rope(face);
+            m = leaf;
+            rho = __uint_as_float(a.x);
+            x += (d + eps) * kx; y += (d + eps) * ky; z += (d + eps) * kz;
+            int next = (rp == -1) ? -1 : TreeStepper<float>::descend(g, rp, x, y, z);
+            if (next >= 0) {
+                load(g, next);
+                if (!inside(g, x, y, z)) {
+                    next = TreeStepper<float>::locate(g, x, y, z); fallbacks++;
+                    if (next >= 0) load(g, next);
+                }
+            } else if (rp != -1) {
+                next = TreeStepper<float>::locate(g, x, y, z); fallbacks++;
+                if (next >= 0) load(g, next);
+            }
+            if (next == leaf) {                    // stuck (TreeDustGrid.cpp:476-493)
+                x = nextafterf(x, (kx < 0.f) ? -FLT_MAX : FLT_MAX);
+                y = nextafterf(y, (ky < 0.f) ? -FLT_MAX : FLT_MAX);
+                z = nextafterf(z, (kz < 0.f) ? -FLT_MAX : FLT_MAX);
+                next = TreeStepper<float>::locate(g, x, y, z);
+                if (next == leaf) next = -1;
+                else if (next >= 0) load(g, next);
+            }
+            if (next < 0) done = true;
+            else { leaf = next; d += eps; }
             if (d > 0.f) { ds = d; return true; }
         }
         return false;
@@ -610,6 +793,7 @@ struct VoronoiStepper {
     int steps;
     int fallbacks;
     int scanned;
+    SKG_D int nscanned() const { return scanned; }
     int cell0;
     static constexpr float rho = -1.f;
 

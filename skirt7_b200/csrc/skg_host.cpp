@@ -303,6 +303,90 @@ void Tree::build(int min_level, int max_level, double max_mass_fraction, double 
 }
 
 // ---------------------------------------------------------------------------------------------
+// Lattice form of the rope tree (layout in skg_tree.h).  Every node box must be an interval of the
+// root's extent halved l_a times along each axis a (l_a <= 20); the codes are checked against the
+// FP64 boxes to 1e-6 of the node width.  Leaves are re-ordered by cell number, so that a leaf
+// reference is the cell number and the record carries no separate cell field; leaf references in
+// the ropes and internal records are translated accordingly.  Leaves the form unchanged (64-byte
+// records) when a box does not fit or the references do not fit 25 bits.
+static void build_lattice_records(const skg_grid& g, const std::vector<int>& order, const std::vector<int>& ref,
+                                  int nleaf, int nint, RopeTree& out) {
+    const int n = g.nnodes;
+    const double org[3] = {g.xmin, g.ymin, g.zmin};
+    const double wid[3] = {g.xmax - g.xmin, g.ymax - g.ymin, g.zmax - g.zmin};
+    if (nleaf >= (1 << 25) || nint >= (1 << 25) - 1) return;
+    std::vector<uint32_t> code(3 * (size_t)n);
+    for (int l = 0; l < n; l++) {
+        const double* b = g.node_box + 6 * (size_t)l;
+        for (int a = 0; a < 3; a++) {
+            const double w = b[a + 3] - b[a];
+            if (!(w > 0) || !(wid[a] > 0)) return;
+            const int lev = (int)std::lround(std::log2(wid[a] / w));
+            if (lev < 0 || lev > 20) return;
+            const double unit = std::ldexp(wid[a], -lev);
+            const long long i = std::llround((b[a] - org[a]) / unit);
+            if (i < 0 || i >= (1ll << lev)) return;
+            const double tol = 1e-6 * unit;
+            if (std::fabs(b[a] - (org[a] + (double)i * unit)) > tol ||
+                std::fabs(b[a + 3] - (org[a] + (double)(i + 1) * unit)) > tol) return;
+            code[3 * (size_t)l + a] = (uint32_t)((2 * i + 1) << (20 - lev));
+        }
+    }
+    std::vector<int> leaf_cell(nleaf, -1);
+    std::vector<char> seen(nleaf, 0);
+    for (int l = 0; l < n; l++) {
+        if (g.node_child[l] >= 0) continue;
+        const int c = g.node_cell[l];
+        if (c < 0 || c >= nleaf || seen[c]) return;      // cells must number the leaves 0..nleaf-1
+        seen[c] = 1;
+        leaf_cell[ref[l]] = c;
+    }
+    auto cref = [&](int r) { return r >= 0 ? leaf_cell[r] : r; };
+    auto as_i = [](float f) { int v; std::memcpy(&v, &f, 4); return v; };
+    auto as_f = [](int v) { float f; std::memcpy(&f, &v, 4); return f; };
+    for (int a = 0; a < 3; a++) {
+        out.lorg[a] = (float)org[a];
+        out.lunit[a] = std::ldexp((float)wid[a], -21);
+    }
+    out.prec.assign(2 * (size_t)nleaf, uint4{0, 0, 0, 0});
+    for (int l : order) {
+        const uint32_t* c = code.data() + 3 * (size_t)l;
+        if (g.node_child[l] >= 0) {
+            const int j = -ref[l] - 2;
+            float4& h = out.irec[3 * (size_t)j];
+            // the split point is the node's centre, as the walls of its children compute it
+            h.x = std::fmaf((float)c[0], out.lunit[0], out.lorg[0]);
+            h.y = std::fmaf((float)c[1], out.lunit[1], out.lorg[1]);
+            h.z = std::fmaf((float)c[2], out.lunit[2], out.lorg[2]);
+            for (int q = 1; q <= 2; q++) {
+                float4& v = out.irec[3 * (size_t)j + q];
+                v = float4{as_f(cref(as_i(v.x))), as_f(cref(as_i(v.y))), as_f(cref(as_i(v.z))), as_f(cref(as_i(v.w)))};
+            }
+            continue;
+        }
+        const int li = ref[l], cell = leaf_cell[li];
+        const float4 r03 = out.lrec[4 * (size_t)li + 2], r45 = out.lrec[4 * (size_t)li + 3];
+        const int rope[6] = {as_i(r03.x), as_i(r03.y), as_i(r03.z), as_i(r03.w), as_i(r45.x), as_i(r45.y)};
+        uint32_t bits[5] = {0, 0, 0, 0, 0};
+        for (int w = 0; w < 6; w++) {
+            const int r = rope[w];
+            const uint64_t v = (r == -1) ? 0x3FFFFFFull : (r >= 0) ? (uint64_t)leaf_cell[r] : (uint64_t)((1 << 25) + (-r - 2));
+            const int bit = 26 * w, wd = bit >> 5, sh = bit & 31;
+            const uint64_t x = v << sh;
+            bits[wd] |= (uint32_t)x;
+            if (wd + 1 < 5) bits[wd + 1] |= (uint32_t)(x >> 32);
+        }
+        const uint64_t box = (uint64_t)c[0] | ((uint64_t)c[1] << 21) | ((uint64_t)c[2] << 42);
+        out.prec[2 * (size_t)cell] = uint4{0u, (uint32_t)box, (uint32_t)(box >> 32), bits[0]};
+        out.prec[2 * (size_t)cell + 1] = uint4{bits[1], bits[2], bits[3], bits[4]};
+    }
+    out.root_ref = cref(out.root_ref);
+    out.lattice = true;
+    std::vector<float4>().swap(out.lrec);
+    for (int m = 0; m < nleaf; m++) out.cell_leaf[m] = m;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Rope-linked tree for the FP32 walk.
 //
 // Leaves are numbered in depth-first order (children in order: for an octree the Morton order of
@@ -310,7 +394,7 @@ void Tree::build(int min_level, int max_level, double max_mass_fraction, double 
 // leaf face carries a rope: the deepest node beyond the face whose box covers the whole face
 // (Havran's neighbour links).  A step then follows the rope of the exit wall -- to the next leaf
 // directly, or to a node from which the point descends one or two levels.
-void build_rope_tree(const skg_grid& g, RopeTree& out) {
+void build_rope_tree(const skg_grid& g, RopeTree& out, bool allow_lattice) {
     const int n = g.nnodes;
     std::vector<int> ref(n, -1);
     std::vector<int> order;            // depth-first visit order
@@ -388,6 +472,7 @@ void build_rope_tree(const skg_grid& g, RopeTree& out) {
         out.lrec[4 * (size_t)li + 2] = float4{as_f(rope[0]), as_f(rope[1]), as_f(rope[2]), as_f(rope[3])};
         out.lrec[4 * (size_t)li + 3] = float4{as_f(rope[4]), as_f(rope[5]), 0.f, 0.f};
     }
+    if (allow_lattice) build_lattice_records(g, order, ref, nleaf, nint, out);
 }
 
 // Builds the topology from explicit decisions (split[l] for node l in creation order).

@@ -198,10 +198,17 @@ __global__ void embed_density_kernel(float4* lrec, int nleaves, const float* __r
     int cell = __float_as_int(lrec[4 * (size_t)li + 1].w);
     lrec[4 * (size_t)li].w = rhof[cell];
 }
+// The same for the lattice form: word 0 of cell m's 32-byte record.
+__global__ void embed_density_lattice_kernel(uint4* prec, int ncells, const float* __restrict__ rhof) {
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= ncells) return;
+    prec[2 * (size_t)m].x = __float_as_uint(rhof[m]);
+}
 cudaError_t launch_embed_density(const DevGrid& g, const float* rhof, cudaStream_t s) {
     int n = g.ncells;
     if (n <= 0) return cudaSuccess;
-    embed_density_kernel<<<(n + 255) / 256, 256, 0, s>>>(const_cast<float4*>(g.lrec), n, rhof);
+    if (g.lattice) embed_density_lattice_kernel<<<(n + 255) / 256, 256, 0, s>>>(const_cast<uint4*>(g.prec), n, rhof);
+    else embed_density_kernel<<<(n + 255) / 256, 256, 0, s>>>(const_cast<float4*>(g.lrec), n, rhof);
     return cudaGetLastError();
 }
 

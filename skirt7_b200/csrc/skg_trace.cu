@@ -78,6 +78,8 @@ __global__ void optical_depth_kernel(const DevGrid g, const DevScene* __restrict
             if (f64) KERNEL<double, TreeStepper><<<bl, th, 0, s>>>(__VA_ARGS__);                    \
             else if (g.search == SKG_SEARCH_BOOKKEEPING)                                            \
                 KERNEL<float, TreeNodeWalk><<<bl, th, 0, s>>>(__VA_ARGS__);                         \
+            else if (g.lattice)                                                                     \
+                KERNEL<float, TreeLatticeStepper><<<bl, th, 0, s>>>(__VA_ARGS__);                   \
             else KERNEL<float, TreeStepper><<<bl, th, 0, s>>>(__VA_ARGS__);                         \
         }                                                                                           \
         return cudaGetLastError();                                                                  \

@@ -40,6 +40,9 @@ namespace skg {
 #ifndef SKG_TRAV_MIN_BLOCKS
 #define SKG_TRAV_MIN_BLOCKS 4
 #endif
+#ifndef SKG_EVENT_MIN_BLOCKS
+#define SKG_EVENT_MIN_BLOCKS 1
+#endif
 // a lane whose job ended takes the next one when this many lanes of its warp (or all of its live
 // lanes) wait for one: the job start (job, packet record, start leaf: dependent loads) is then paid
 // once for several lanes instead of stalling the warp for each (8 measured fastest of 1-32 on the
@@ -200,7 +203,15 @@ __device__ __noinline__ double peel_weight(const DevScene& S, int ell, int cell,
 
 // Forced interaction optical depth and weight: MonteCarloSimulation::simulatepropagation
 // (:513-531) with Random::exponcutoff (Random.cpp:163-176).  Returns tau; L is reweighted.
-__device__ __noinline__ double sample_interaction(double xi, double taupath, double& L, Philox& rng) {
+#ifndef SKG_SAMPLE_INLINE
+#define SKG_SAMPLE_INLINE 0
+#endif
+#if SKG_SAMPLE_INLINE
+SKG_D
+#else
+__device__ __noinline__
+#endif
+double sample_interaction(double xi, double taupath, double& L, Philox& rng) {
     auto expcut = [&](double xmax) -> double {
         if (xmax < 1e-10) return rng.uniform() * xmax;
         double x;
@@ -272,7 +283,7 @@ SKG_D int peel_jobs(const DevScene& S, int ell, bool scat, int cell, double kx, 
 constexpr int SED_PRIV = 1024;          // SED bins a block keeps privately (8 KB)
 
 template<typename R>
-__global__ void __launch_bounds__(256) event_kernel(const WaveParams W) {
+__global__ void __launch_bounds__(256, SKG_EVENT_MIN_BLOCKS) event_kernel(const WaveParams W) {
     __shared__ unsigned long long s_cnt[C_N];
     __shared__ double s_sed[SED_PRIV];
     const RunParams& P = W.R;
@@ -438,7 +449,8 @@ __global__ void __launch_bounds__(256) event_kernel(const WaveParams W) {
 
 // End of the packet's own path (simulateescapeandabsorption :441-462, the termination test of
 // dostellaremissionchunk :283, simulatepropagation :513-531).  Returns 1 when the path must be
-// re-walked to tau_int, 0 when the packet record is complete, -1 on an error.  Inlined: as a call
+// re-walked to tau_int (the packet's luminosity is then already in its record), 0 when the packet
+// record is complete, -1 on an error.  Inlined: as a call
 // it made the traversal kernel keep a 264-byte stack frame for the call's saved registers (88
 // bytes inlined; the traversal pass ran 11 % faster).
 SKG_D int after_path(const WaveParams& W, const DevScene& S, int p, int phase, int ell,
@@ -467,6 +479,7 @@ SKG_D int after_path(const WaveParams& W, const DevScene& S, int p, int phase, i
     rng.c0 = K.rngc;
     tau_int = sample_interaction(S.xi, taupath, L, rng);
     K.rngc = rng.c0;
+    K.L = L;                              // the weight the packet carries to its interaction point
     return 1;
 }
 
@@ -488,8 +501,11 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
     int j = -1;                       // the lane's job (-1: none)
     int p = 0, slot = 0, ell = 0;
     int kind = 0;                     // 0 peel-off, 1 path, 2 re-walk to the interaction point
-    double tau = 0, s = 0, tau_int = 0, L = 0, Lsca = 0;
-    double kext1 = -1.0;              // kappa_ext at the job's wavelength (one dust component), else -1
+    double tau = 0;                   // optical depth walked
+    // values of one job kind share two registers -- path: v1 = L, v2 = L_sca (several dust
+    // components); re-walk: v1 = path length walked, v2 = the interaction optical depth
+    double v1 = 0, v2 = 0;
+    float kext1 = -1.f;               // kappa_ext at the job's wavelength (one dust component), else -1
     Stepper<R> st;
     unsigned c_steps = 0;
 
@@ -514,17 +530,15 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
                 slot = P.items[K.item].slot;
                 const DevScene& S = *s_scene[slot];
                 const int hint = K.pos_cell;
-                kext1 = (S.ncomp == 1) ? S.kext[ell] : -1.0;
+                kext1 = (S.ncomp == 1) ? (float)S.kext[ell] : -1.f;
                 R kx, ky, kz;
-                if (jb.y == JOB_MAIN) { kx = (R)K.kx; ky = (R)K.ky; kz = (R)K.kz; kind = 1; L = K.L; Lsca = 0; }
+                if (jb.y == JOB_MAIN) { kx = (R)K.kx; ky = (R)K.ky; kz = (R)K.kz; kind = 1; v1 = K.L; v2 = 0; }
                 else { kx = (R)S.gkx[jb.y]; ky = (R)S.gky[jb.y]; kz = (R)S.gkz[jb.y]; kind = 0; }
                 st.init(sg[slot], (R)K.x, (R)K.y, (R)K.z, kx, ky, kz, hint);
                 if (kind == 1 && hint == -2) W.pk[p].pos_cell = st.cell0;
-                tau = 0; s = 0;
-                // entry segments outside the grid (m = -1) carry no optical depth: only their
-                // length counts (for the re-walk)
-                R d0;
-                while (st.pd.pop(d0)) s += (double)d0;
+                tau = 0;
+                // entry segments outside the grid (m = -1) carry no optical depth: only the
+                // re-walk, which measures length, takes them
             }
         }
 
@@ -537,7 +551,7 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
         if (st.walk(g, m, ds)) {
             c_steps++;
             // one dust component: the FP32 tree walk carries the cell density in its leaf record
-            const double kr = (kext1 >= 0.0 && st.rho >= 0.f) ? kext1 * (double)st.rho : kappa_rho<R>(S, m, ell);
+            const double kr = (kext1 >= 0.f && st.rho >= 0.f) ? (double)(kext1 * st.rho) : kappa_rho<R>(S, m, ell);
             const double dtau = kr * (double)ds;
             if (kind == 0) {
                 tau += dtau;
@@ -546,7 +560,7 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
                     const bool store = (phase == SKG_PHASE_STELLAR) ? (S.store_abs != 0) : (phase == SKG_PHASE_DUST_SELFABS);
                     if (S.ncomp == 1) {
                         if (store) {
-                            const double Lintm = L * exp(-tau) * (-expm1(-dtau));
+                            const double Lintm = v1 * exp(-tau) * (-expm1(-dtau));
                             double* labs = (phase == SKG_PHASE_STELLAR) ? S.labs_stel : S.labs_dust;
                             atomicAdd(labs + (size_t)m * S.nlambda + ell, (1.0 - S.albedo[ell]) * Lintm);
                             atomicAdd(&s_cnt[C_ABS], 1ull);
@@ -558,8 +572,8 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
                             ksca += rh * S.ksca[h * S.nlambda + ell]; kext += rh * S.kext[h * S.nlambda + ell];
                         }
                         const double alb = (kext > 0.0) ? ksca / kext : 0.0;
-                        const double Lintm = L * exp(-tau) * (-expm1(-dtau));
-                        Lsca += alb * Lintm;
+                        const double Lintm = v1 * exp(-tau) * (-expm1(-dtau));
+                        v2 += alb * Lintm;
                         if (store) {
                             double* labs = (phase == SKG_PHASE_STELLAR) ? S.labs_stel : S.labs_dust;
                             atomicAdd(labs + (size_t)m * S.nlambda + ell, (1.0 - alb) * Lintm);
@@ -569,38 +583,38 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
                 }
                 tau += dtau;
             } else {
-                const double tn = tau + dtau, sn = s + (double)ds;
-                if (tn > tau_int) {
+                const double tn = tau + dtau, sn = v1 + (double)ds;
+                if (tn > v2) {
                     Packet& K = W.pk[p];
-                    K.L = L;
-                    K.s_int = s + ((tau_int - tau) / (tn - tau)) * (sn - s);
+                    K.s_int = v1 + ((v2 - tau) / (tn - tau)) * (sn - v1);
                     K.int_cell = m;
                     K.state = PK_INTERACT;
                     atomicAdd(&s_cnt[C_TRAV], 1ull);
-                    atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.scanned);
+                    atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.nscanned());
                     atomicAdd(&s_cnt[C_FB], (unsigned long long)st.fallbacks);
                     j = -1;
                 } else {
-                    tau = tn; s = sn;
+                    tau = tn; v1 = sn;
                 }
             }
         } else {
             // the traversal reached the edge of the grid
             atomicAdd(&s_cnt[C_TRAV], 1ull);
-            atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.scanned);
+            atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.nscanned());
             atomicAdd(&s_cnt[C_FB], (unsigned long long)st.fallbacks);
             if (st.steps > g.max_steps) { atomicOr(P.err, ERR_STEP_BUDGET); atomicAdd(&s_cnt[C_ERR], 1ull); }
             if (kind == 0) {
                 W.jtau[j] = tau;
                 j = -1;
             } else if (kind == 1) {
-                const int rc = after_path(W, S, p, phase, ell, tau, Lsca, L, tau_int);
+                double L = v1, tau_int = 0;
+                const int rc = after_path(W, S, p, phase, ell, tau, v2, L, tau_int);
                 if (rc == 1) {
                     const Packet& K = W.pk[p];
                     st.init(g, (R)K.x, (R)K.y, (R)K.z, (R)K.kx, (R)K.ky, (R)K.kz, K.pos_cell);
-                    tau = 0; s = 0; kind = 2;
+                    tau = 0; v1 = 0; v2 = tau_int; kind = 2;
                     R d0;
-                    while (st.pd.pop(d0)) s += (double)d0;
+                    while (st.pd.pop(d0)) v1 += (double)d0;
                 } else {
                     if (rc < 0) atomicAdd(&s_cnt[C_ERR], 1ull);
                     j = -1;
@@ -608,7 +622,7 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
             } else {
                 // DustGridPath::pathlength: an optical depth beyond the last segment gives the full length
                 Packet& K = W.pk[p];
-                K.L = L; K.s_int = s; K.int_cell = -1; K.state = PK_INTERACT;
+                K.s_int = v1; K.int_cell = -1; K.state = PK_INTERACT;
                 j = -1;
             }
         }
@@ -647,7 +661,7 @@ cudaError_t enqueue_wave(const WaveParams& W, int nslots, int trav_blocks, cudaE
 
 using WaveFn = cudaError_t (*)(const WaveParams&, int, int, cudaEvent_t, cudaStream_t);
 
-WaveFn pick(int grid_type, bool bookkeeping, int precision) {
+WaveFn pick(int grid_type, int tree_walk, int precision) {
     const bool f64 = precision == SKG_PREC_FP64;
     switch (grid_type) {
     case SKG_GRID_CARTESIAN:
@@ -655,7 +669,9 @@ WaveFn pick(int grid_type, bool bookkeeping, int precision) {
     case SKG_GRID_OCTREE:
     case SKG_GRID_BINTREE:
         if (f64) return enqueue_wave<double, TreeStepper>;
-        return bookkeeping ? enqueue_wave<float, TreeNodeWalk> : enqueue_wave<float, TreeStepper>;
+        if (tree_walk == TW_NODES) return enqueue_wave<float, TreeNodeWalk>;
+        if (tree_walk == TW_LATTICE) return enqueue_wave<float, TreeLatticeStepper>;
+        return enqueue_wave<float, TreeStepper>;
     default:
         return f64 ? enqueue_wave<double, VoronoiStepper> : enqueue_wave<float, VoronoiStepper>;
     }
@@ -702,7 +718,7 @@ cudaError_t WaveRunner::reserve(size_t pool, int ngroups) {
 }
 
 cudaError_t WaveRunner::enqueue(int n) {
-    WaveFn fn = pick(grid_type_, bookkeeping_, precision_);
+    WaveFn fn = pick(grid_type_, tree_walk_, precision_);
     cudaError_t e;
     for (int i = 0; i < n; i++) {
         const int w = waves_ + i, b = w & 1;
@@ -732,10 +748,10 @@ cudaError_t WaveRunner::enqueue(int n) {
                                              : cudaEventRecordWithFlags(copied_, stream_, cudaEventRecordExternal);
 }
 
-cudaError_t WaveRunner::begin(const RunParams& P, int grid_type, bool bookkeeping, int precision, int nslots,
+cudaError_t WaveRunner::begin(const RunParams& P, int grid_type, int tree_walk, int precision, int nslots,
                               size_t npool, int trav_blocks, cudaStream_t s) {
     if (npool == 0 || npool > cap_pool_) return cudaErrorInvalidValue;
-    P_ = P; grid_type_ = grid_type; bookkeeping_ = bookkeeping; precision_ = precision; nslots_ = nslots;
+    P_ = P; grid_type_ = grid_type; tree_walk_ = tree_walk; precision_ = precision; nslots_ = nslots;
     trav_blocks_ = trav_blocks; stream_ = s; npool_ = (int)npool; waves_ = 0;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(s, &cs);

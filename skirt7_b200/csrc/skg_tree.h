@@ -53,12 +53,29 @@ struct Tree {
 //   irec: 3 float4 per internal node: (split x, y, z, int split direction or -1 for an octree node),
 //         then 8 int child references
 //   references: >= 0 leaf index, -1 none (outside the domain), <= -2 internal node -(ref + 2)
+//
+// Lattice form, for trees whose nodes all split at their midpoints (OctTreeNode, BinTreeNode): a
+// node's extent along axis a is the interval of level l_a and index i_a of the root's extent, coded
+// as the 21-bit centre c_a = (2 i_a + 1) << (20 - l_a) in units u_a = extent_a / 2^21, so that
+// every wall is fmaf(integer, u_a, origin_a) -- the same float on both sides of it.
+//   prec: 2 uint4 (32 bytes) per leaf, in cell-number order (leaf reference = cell number)
+//     word 0      density (float bits; 0 until embedded)
+//     words 1-2   codes: bits 0-20 c_x, 21-41 c_y, 42-62 c_z of the 64-bit word (w2:w1)
+//     words 3-7   ropes of walls 0..5, 26 bits each at bit 26*wall of the 160-bit string
+//                 (0x3FFFFFF none, < 2^25 cell number, else internal node + 2^25)
+//   irec as above, with leaf references replaced by cell numbers and split points computed as
+//   fmaf(c, u, origin) from the node's centre codes.
 struct RopeTree {
     std::vector<float4> lrec, irec;
     std::vector<int> cell_leaf;
     int root_ref = -1;
+    bool lattice = false;
+    std::vector<uint4> prec;
+    float lorg[3] = {0, 0, 0}, lunit[3] = {0, 0, 0};
 };
-void build_rope_tree(const skg_grid& g, RopeTree& out);
+// Builds the lattice form when every node fits the lattice (and allow_lattice), else the 64-byte
+// leaf records.
+void build_rope_tree(const skg_grid& g, RopeTree& out, bool allow_lattice = true);
 
 }  // namespace skg
 

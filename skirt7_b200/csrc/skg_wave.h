@@ -24,8 +24,9 @@ public:
     // ngroups peel-off groups at most per packet.
     cudaError_t reserve(size_t pool, int ngroups);
     // Enqueues the reset of the pool and the first waves of a phase on stream s.  P holds the
-    // staged tables; nslots the slots whose DevGrid the traversal pass keeps in shared memory.
-    cudaError_t begin(const RunParams& P, int grid_type, bool bookkeeping, int precision, int nslots,
+    // staged tables; nslots the slots whose DevGrid the traversal pass keeps in shared memory;
+    // tree_walk the FP32 tree walk (TreeWalk) of tree grids.
+    cudaError_t begin(const RunParams& P, int grid_type, int tree_walk, int precision, int nslots,
                       size_t npool, int trav_blocks, cudaStream_t s);
     // Waits for the enqueued waves and enqueues more until no packet is left; then records
     // `end` (if given) on the phase's stream.  timeout_ms < 0 waits without limit.
@@ -60,7 +61,7 @@ private:
     cudaStream_t stream_ = nullptr;
     RunParams P_{};
     int grid_type_ = 0, precision_ = 0, nslots_ = 1, trav_blocks_ = 0;
-    bool bookkeeping_ = false;
+    int tree_walk_ = TW_ROPE;
     int npool_ = 0;
     int waves_ = 0;
     std::vector<cudaEvent_t> ev_;      // 3 per wave: before the event pass, between, after the traversal

@@ -197,3 +197,45 @@ def test_tree_fp64_bit_exact(orc, gtype, search):
     assert np.mean(err < 2e-6 * diag + 1e-5 * L64) > 0.999
     assert np.max(err) < 1e-4 * diag
     ctx.close()
+
+
+@pytest.mark.parametrize("gtype", [A.GRID_OCTREE, A.GRID_BINTREE])
+def test_tree_fp32_lattice_records_against_rope_records(gtype, monkeypatch):
+    """The FP32 walk on 32-byte lattice leaf records (walls computed from integer centre codes)
+    against the walk on 64-byte records holding the FP32-rounded FP64 boxes: the walls differ by at
+    most an FP32 rounding, so cell sequences agree except at near-ties and path lengths and optical
+    depths agree to FP32 resolution."""
+    ext = (-20 * KPC, -20 * KPC, -2 * KPC, 20 * KPC, 20 * KPC, 2 * KPC)
+    split = _random_splits(gtype, 7, 2, 0.35, seed=1) if gtype == A.GRID_OCTREE else _random_splits(gtype, 22, 6, 0.62, seed=1)
+    tree = runtime.tree_from_splits(gtype, ext, split, A.SEARCH_NEIGHBOR)
+    assert tree.ncells > 3000
+    m = models.oligo_disk()
+    m.dustGrid = tree
+    m.rho = np.random.default_rng(4).uniform(0.5e-21, 2e-21, (1, tree.ncells))
+    r, k = seeded_rays(200000, ext, seed=8, disk=(4 * KPC, 0.35 * KPC))
+    monkeypatch.setenv("SKG_TREE_RECORDS", "rope")
+    ctx_rope = runtime.Context(m)
+    monkeypatch.delenv("SKG_TREE_RECORDS")
+    ctx_lat = runtime.Context(m)
+    oa, ca, da = ctx_rope.trace_paths(r, k, A.PREC_FP32)
+    ob, cb, db = ctx_lat.trace_paths(r, k, A.PREC_FP32)
+    assert not (np.array_equal(oa, ob) and np.array_equal(da, db)), "both contexts walked the same records"
+    # rays with identical cell sequences
+    na, nb = np.diff(oa), np.diff(ob)
+    same = na == nb
+    ids = np.flatnonzero(same & (na > 0))
+    seq_ok = np.array([np.array_equal(ca[oa[i]:oa[i + 1]], cb[ob[i]:ob[i + 1]]) for i in ids[:20000]])
+    assert np.mean(same) > 0.999 and np.mean(seq_ok) > 0.999, (np.mean(same), np.mean(seq_ok))
+    nz = na > 0
+    assert np.array_equal(nz, nb > 0)
+    La = np.add.reduceat(da, oa[:-1][nz])
+    Lb = np.add.reduceat(db, ob[:-1][nz])
+    diag = np.sqrt(40.0 ** 2 + 40.0 ** 2 + 4.0 ** 2) * KPC
+    assert np.max(np.abs(La - Lb)) < 1e-5 * diag
+    ta = ctx_rope.optical_depth(r, k, 0, A.PREC_FP32)
+    tb = ctx_lat.optical_depth(r, k, 0, A.PREC_FP32)
+    ok = ta > 1e-3
+    rel = np.abs(ta[ok] - tb[ok]) / ta[ok]
+    assert np.mean(rel < 1e-5) > 0.999 and abs(tb[ok].sum() / ta[ok].sum() - 1) < 1e-6
+    ctx_rope.close()
+    ctx_lat.close()

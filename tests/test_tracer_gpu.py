@@ -57,10 +57,14 @@ def _well_sampled(zok, O, f):
 
 
 def _check(z, ok, what, zmax=5.0, frac=0.03):
+    """z of batch means (16 + 16 batches: Student-t tails, P(|z| > 3) about 0.5 %); the oracle's
+    batches vary from run to run (its threads take chunks dynamically, as the reference's do), so
+    the count beyond 3 sigma gets two elements of slack above frac of the elements tested."""
     zz = np.abs(z[ok])
     assert zz.size > 0, what
     assert zz.max() < zmax, "%s: max |z| = %.2f" % (what, zz.max())
-    assert np.mean(zz > 3) < frac, "%s: %.3f of elements beyond 3 sigma" % (what, np.mean(zz > 3))
+    nbeyond = int(np.sum(zz > 3))
+    assert nbeyond <= frac * zz.size + 2, "%s: %d of %d elements beyond 3 sigma" % (what, nbeyond, zz.size)
 
 
 @pytest.mark.parametrize("precision", [A.PREC_FP32, A.PREC_FP64])
