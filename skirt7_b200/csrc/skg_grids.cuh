@@ -750,6 +750,9 @@ struct TreeLatticeStepper<float> {
 
 // =============================================================================================
 // Voronoi
+#ifndef SKG_VOR_NODIV
+#define SKG_VOR_NODIV 1
+#endif
 template<typename R> SKG_D V3<R> site_pos(const DevGrid& g, int m);
 template<> SKG_D V3<double> site_pos<double>(const DevGrid& g, int m) {
     const double* p = g.site + 3 * (size_t)m; return mk3(p[0], p[1], p[2]);
@@ -879,9 +882,23 @@ SKG_D bool VoronoiStepper<float>::walk(const DevGrid& g, int& m, float& ds) {
     if (qe < 0 && !done) { qb = g.vnoff[mr]; qe = g.vnoff[mr + 1]; }
     while (!done) {
         if (++steps > g.max_steps) { done = true; return false; }
-        float sq = FLT_MAX;
         int qbest = -1;
         const int q0 = qb, q1 = qe;
+#if SKG_VOR_NODIV
+        // the nearest wall ahead without a division per entry: a candidate s = num/den (den =
+        // n.k > 0) is nearer than the best so far when num * bden < bnum * den
+        float bnum = 1.f, bden = 0.f;
+#pragma unroll 4
+        for (int q = q0; q < q1; q++) {
+            const float4 pl = __ldg(g.vplane + q);
+            const float den = pl.x * kx + pl.y * ky + pl.z * kz;
+            const float num = pl.w - (pl.x * x + pl.y * y + pl.z * z);
+            if (den > 0.f && num > 0.f && num * bden < bnum * den) { bnum = num; bden = den; qbest = q; }
+        }
+        scanned += q1 - q0;
+        const float sq = (qbest >= 0) ? bnum / bden : FLT_MAX;
+#else
+        float sq = FLT_MAX;
 #pragma unroll 4
         for (int q = q0; q < q1; q++) {
             float4 pl = __ldg(g.vplane + q);
@@ -892,6 +909,7 @@ SKG_D bool VoronoiStepper<float>::walk(const DevGrid& g, int& m, float& ds) {
                 if (si > 0.f && si < sq) { sq = si; qbest = q; }
             }
         }
+#endif
         if (qbest < 0) {
             x += kx * g.epsf; y += ky * g.epsf; z += kz * g.epsf;
             mr = voronoi_cell_index<float>(g, x, y, z);
