@@ -721,10 +721,19 @@ struct TreeLatticeStepper<float> {
             m = leaf;
             rho = __uint_as_float(a.x);
             x += (d + eps) * kx; y += (d + eps) * ky; z += (d + eps) * kz;
+            // The rope's node covers the whole exit face: when the point lies beyond (or on) the
+            // exit wall and, along the other axes, still within the walls ahead of it, the leaf it
+            // descends to holds it and the containment test can be skipped (the point crossed
+            // near an edge or a corner otherwise).
+            const int ax = face >> 1;
+            const bool bx = (kx < 0.f) ? (x <= xnext) : (x >= xnext), wx = (kx < 0.f) ? (x >= xnext) : (x <= xnext);
+            const bool by = (ky < 0.f) ? (y <= ynext) : (y >= ynext), wy = (ky < 0.f) ? (y >= ynext) : (y <= ynext);
+            const bool bz = (kz < 0.f) ? (z <= znext) : (z >= znext), wz = (kz < 0.f) ? (z >= znext) : (z <= znext);
+            const bool on_face = (ax == 0 ? bx : wx) && (ax == 1 ? by : wy) && (ax == 2 ? bz : wz);
             int next = (rp == -1) ? -1 : TreeStepper<float>::descend(g, rp, x, y, z);
             if (next >= 0) {
                 load(g, next);
-                if (!inside(g, x, y, z)) {
+                if (!on_face && !inside(g, x, y, z)) {
                     next = TreeStepper<float>::locate(g, x, y, z); fallbacks++;
                     if (next >= 0) load(g, next);
                 }
