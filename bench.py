@@ -183,6 +183,12 @@ class Workload:
             b = c["steps"] * 28 * f + c["nbr_scanned"] * 4
         return b + 8 * c["absorb_adds"]
 
+    # DRAM bytes per cell step of the traversal pass, measured with ncu
+    # (dram__bytes_read.sum + dram__bytes_write.sum summed over every traversal launch of one
+    # stellar phase, divided by the phase's cell steps; profiles/traffic_per_step.md), FP32 walk
+    NCU_DRAM_BYTES_PER_STEP = {"octree_pan": 11.37, "cartesian_oligo": 3.40, "voronoi_clumpy": 268.05,
+                               "kdtree_dust": 49.15}
+
     def frames(self):
         from skirt7_b200 import _abi as A
         return [i for i, ins in enumerate(self.model.instruments) if ins.type != A.INSTR_SED]
@@ -236,7 +242,7 @@ def run_reference(args, rank, world):
     # calibrate the sample to about --cpu-seconds per step
     probe = oracle.simulate(model, args.packets * args.gpus, nthreads=threads, seed=1, max_packets=2000, **kw)
     rate = probe["stats"]["packets"] / max(probe["stats"]["seconds"], 1e-6)
-    sample = int(max(1000, min(2e6, rate * args.cpu_seconds)))
+    sample = int(max(1000, min(5e6, rate * args.cpu_seconds)))
     vals = []
     for s in range(args.warmup + args.steps):
         r = oracle.simulate(model, args.packets * args.gpus, nthreads=threads, seed=100 + s, max_packets=sample, **kw)
@@ -382,6 +388,8 @@ def main():
     ev_ms, trav_ms, waves = ctx.phase_times()
     c = ctx.counters()
     alg_bytes = wl.alg_bytes(c, prec == A.PREC_FP32)
+    bps = wl.NCU_DRAM_BYTES_PER_STEP.get(wl.name) if prec == A.PREC_FP32 else None
+    traffic = bps * c["steps"] / max(waves, 1) if bps else None
     peak, peak_kind = peaks()
     achieved = alg_bytes / (trav_ms / 1e3) / 1e9 if trav_ms > 0 else 0.0
 
@@ -421,18 +429,23 @@ def main():
         line = {
             "metric": wl.metric,
             "value": value, "unit": "packets/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": total_ms / args.steps, "ms_steps": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if prec == A.PREC_FP32 else "f64", "data": "synthetic",
             "config": _config(args, wl),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "trav_kernel (traversal pass of the stellar phase)",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "traffic_basis": ("ncu DRAM bytes per cell step of this workload's traversal pass "
+                                           "(%.2f B, profiles/traffic_per_step.md) x this phase's cell steps per "
+                                           "traversal pass" % bps) if bps else None,
+                         "kernel": "trav_kernel, path and peel-off instantiations (traversal pass of the stellar phase)",
+                         "launch": "one traversal pass of a wave (its path-job and peel-off-job kernels)",
                          "algorithmic_bytes_per_launch": alg_bytes / max(waves, 1),
                          "kernel_ms_per_launch": trav_ms / max(waves, 1), "launches_per_phase": waves,
                          "phase_ms": kms, "event_pass_ms": ev_ms, "traversal_pass_ms": trav_ms},
             "e2e": {"value": e2e, "unit": "packets/s", "h2d_bytes_per_step": len(phases) * (4 * nl + 64),
                     "d2h_bytes_per_step": cubes_bytes},
-            "gpu_launches": 2 * waves * len(phases) * args.steps,
+            # per wave: the event pass and the two traversal kernels (path jobs, peel-off jobs)
+            "gpu_launches": 3 * waves * len(phases) * args.steps,
             "clocks": clk,
             "counters_stellar_phase": c,
         }
@@ -486,12 +499,13 @@ def cpu_baseline(args, wl, ctx):
     kw = dict(dust_emission_phase=wl.dust_phase)
     probe = oracle.simulate(model, args.packets, nthreads=threads, seed=1, max_packets=2000, **kw)
     rate = probe["stats"]["packets"] / max(probe["stats"]["seconds"], 1e-6)
-    sample = int(max(1000, min(2e6, rate * args.cpu_seconds)))
+    sample = int(max(1000, min(5e6, rate * args.cpu_seconds)))
     r = oracle.simulate(model, args.packets, nthreads=threads, seed=2, max_packets=sample, **kw)
     model.rho = None
     return {"value": r["stats"]["packets"] / r["stats"]["seconds"], "unit": "packets/s", "cores": threads,
-            "kind": "port", "sample": "%d packets over all %d wavelengths (%.1f s)" %
-                                      (r["stats"]["packets"], model.wavelengthGrid.Nlambda, r["stats"]["seconds"])}
+            "kind": "port", "sample": "%d packets over all %d wavelengths%s (%.1f s of packet loops)" %
+                                      (r["stats"]["packets"], model.wavelengthGrid.Nlambda,
+                                       ", both phases" if wl.dust_phase else "", r["stats"]["seconds"])}
 
 
 if __name__ == "__main__":

@@ -1440,13 +1440,13 @@ int orc_sample_density(const skg_scene* sc, int nthreads, uint64_t seed, double*
 // MonteCarloSimulation.cpp:241-295) for `packages` per wavelength, optionally followed by
 // `selfabs_cycles` dust self-absorption cycles (fixed cycle count, PanMonteCarloSimulation.cpp:106-242,
 // one stage) and the dust emission phase (:246-346).  If max_packets > 0 only that many
-// packets of the stellar phase run (a bounded sample for timing); Npp is unchanged so that the
-// per-packet luminosity stays that of the full run.
+// packets of each phase run (a bounded sample for timing); Npp is unchanged so that the
+// per-packet luminosity stays that of the full run.  st->seconds is the time of the packet loops
+// of the phases (as the reference's TimeLogger times a phase), without the set-up.
 // cubes[i]/seds[i] receive instrument i's tallies (layout of skg_read_instrument).
 int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t seed, int selfabs_cycles,
                  int dust_emission_phase, int64_t max_packets, double** cubes, double** seds,
                  double* labs_stel, double* labs_dust, double* temperature, orc_stats* st) {
-    auto t0 = std::chrono::steady_clock::now();
     Sim* S = buildSim(sc);
     Sim& R = *S;
     size_t nc = R.grid->ncells;
@@ -1456,6 +1456,8 @@ int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t se
     uint64_t Nchunks, chunksize, Npp;
     chunkParams(packages, nthreads, 1, nl, Nchunks, chunksize, Npp);
     std::atomic<int64_t> launched{0};
+    double loop_seconds = 0;
+    const auto t_loop = std::chrono::steady_clock::now();
 
     // stellar emission (MonteCarloSimulation.cpp:259-295)
     parallelCall(nthreads, (uint64_t)nl*Nchunks, seed, [&](uint64_t index, Rng& rng) {
@@ -1471,6 +1473,7 @@ int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t se
             if (pp.L > 0) lifecycle(R, pp, path, ppath, rng, Lthreshold, R.storeAbs, true);
         }
     });
+    loop_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t_loop).count();
 
     // dust self-absorption cycles and dust emission (PanMonteCarloSimulation.cpp:106-346)
     auto dustPhase = [&](double pk, bool selfabs) {
@@ -1491,6 +1494,8 @@ int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t se
             if (Ltot > 0) cdf(cums[ell], Lv);
             for (size_t m = 0; m < nc; m++) Lvs[(size_t)ell*nc + m] = Lv[m];
         }
+        std::atomic<int64_t> emitted{0};
+        const auto t_dust = std::chrono::steady_clock::now();
         parallelCall(nthreads, (uint64_t)nl*nch, seed + 7919*(selfabs ? 1 : 2), [&](uint64_t index, Rng& rng) {
             int ell = index % nl;
             double Ltot = Ltots[ell];
@@ -1500,6 +1505,7 @@ int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t se
             double Lmean = Ltot/nc, Lem = Ltot/npp, Lth = Lem/R.minWeightReduction;
             double xi = R.dustEmissionBias;
             for (uint64_t i = 0; i < csz; i++) {
+                if (max_packets > 0 && emitted.fetch_add(1) >= max_packets) return;
                 int m; double weight = 1.0;
                 double X = rng.uniform();
                 if (selfabs) m = locate_clip(Xv.data(), nc+1, X);                 // :219-220
@@ -1515,6 +1521,7 @@ int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t se
                 lifecycle(R, pp, path, ppath, rng, Lth, selfabs, !selfabs);
             }
         });
+        loop_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t_dust).count();
     };
     if (R.dustEmission && R.ncomp && !R.Tv.empty()) {
         for (int c = 0; c < selfabs_cycles; c++) dustPhase(packages, true);
@@ -1533,7 +1540,7 @@ int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t se
         st->packets = R.stats.packets; st->steps = R.stats.steps; st->traversals = R.stats.traversals;
         st->scatterings = R.stats.scatterings; st->fallbacks = R.stats.fallbacks;
         st->npp = Npp; st->chunks = Nchunks;
-        st->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        st->seconds = loop_seconds;
     }
     delete R.grid; delete S;
     return 0;

@@ -153,7 +153,8 @@ struct WaveParams {
     double* jtau;                     // peel-off optical depth
     double* jL;                       // peel-off luminosity
     unsigned* jcount;                 // [0] path jobs, [1] peel-off jobs, [2] jobs taken by the
-                                      // traversal pass, [3] packets with jobs
+                                      // traversal pass (its path kernel when split), [3] packets
+                                      // with jobs, [4] peel-off jobs taken by a split pass
     // the previous wave's jobs (peel-off detection)
     const int2* pjobs;
     const double* pjtau;

@@ -15,7 +15,8 @@
 //                 scatters, or launches a new packet into a free record; then appends the packet's
 //                 next traversals to the wave's job list (one peel-off job per direction group and
 //                 one path job);
-//   trav_kernel   persistent; each lane takes jobs one after another and walks them:
+//   trav_kernel   persistent, launched twice (the path jobs, then the peel-off jobs in a lean
+//                 instantiation); each lane takes jobs one after another and walks them:
 //                 peel-off  accumulates the optical depth towards an observer
 //                           (DustSystem::opticaldepth, DustSystem.cpp:960-976);
 //                 path      streams kappa*rho*ds into the FP64 cumulative optical depth and the
@@ -39,6 +40,16 @@ namespace skg {
 
 #ifndef SKG_TRAV_MIN_BLOCKS
 #define SKG_TRAV_MIN_BLOCKS 4
+#endif
+// The traversal pass as two kernels: the path jobs, then the peel-off jobs in an instantiation
+// that holds the optical depth alone (no spills at 64 registers).  Octree disk, 10^7 packets:
+// 202.5 ms against 214.2 ms for one kernel over both (Voronoi disk: 1357 against 1421 ms); the
+// peel-off kernel at 5 or 6 blocks per SM (48 or 40 registers, spilling) is slower (219, 240 ms).
+#ifndef SKG_PEEL_MIN_BLOCKS
+#define SKG_PEEL_MIN_BLOCKS 4
+#endif
+#ifndef SKG_SPLIT_TRAV
+#define SKG_SPLIT_TRAV 1
 #endif
 // the event pass at 4 blocks of 256 per SM (64 registers, spilling part of the packet record):
 // its divergent, latency-bound code gains more from the warps than it loses to the spills
@@ -486,8 +497,13 @@ SKG_D int after_path(const WaveParams& W, const DevScene& S, int p, int phase, i
     return 1;
 }
 
-template<typename R, template<typename> class Stepper>
-__global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const WaveParams W) {
+// MODE: 0 every job of the wave; 1 the path jobs only; 2 the peel-off jobs only (a lean
+// instantiation: optical depth alone, no path state)
+template<int MODE> struct TravBlocks { static constexpr int value = SKG_TRAV_MIN_BLOCKS; };
+template<> struct TravBlocks<2> { static constexpr int value = SKG_PEEL_MIN_BLOCKS; };
+
+template<typename R, template<typename> class Stepper, int MODE>
+__global__ void __launch_bounds__(256, TravBlocks<MODE>::value) trav_kernel(const WaveParams W) {
     extern __shared__ unsigned char smem_raw[];
     DevGrid* sg = reinterpret_cast<DevGrid*>(smem_raw);
     __shared__ const DevScene* s_scene[MAX_SLOTS];
@@ -497,7 +513,9 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
     for (int i = threadIdx.x; i < C_N; i += blockDim.x) s_cnt[i] = 0;
     for (int i = threadIdx.x; i < H.nslots; i += blockDim.x) { sg[i] = P.grids[i]; s_scene[i] = P.scenes[i]; }
     __syncthreads();
-    const unsigned nmainj = W.jcount[0], njobs = nmainj + W.jcount[1];
+    const unsigned nmainj = W.jcount[0];
+    const unsigned njobs = MODE == 0 ? nmainj + W.jcount[1] : MODE == 1 ? nmainj : W.jcount[1];
+    unsigned* const taken = W.jcount + (MODE == 2 ? 4 : 2);
     const int phase = H.phase;
     const int lane = threadIdx.x & 31;
 
@@ -505,8 +523,10 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
     int p = 0, slot = 0, ell = 0;
     int kind = 0;                     // 0 peel-off, 1 path, 2 re-walk to the interaction point
     double tau = 0;                   // optical depth walked
-    // values of one job kind share two registers -- path: v1 = L, v2 = L_sca (several dust
-    // components); re-walk: v1 = path length walked, v2 = the interaction optical depth
+    // values of one job kind share two registers -- path: v1 = L e^-tau (the luminosity that
+    // reaches the current cell, kept as a running product: one expm1 per absorbing cell step),
+    // v2 = L_sca (several dust components); re-walk: v1 = path length walked, v2 = the
+    // interaction optical depth
     double v1 = 0, v2 = 0;
     float kext1 = -1.f;               // kappa_ext at the job's wavelength (one dust component), else -1
     unsigned c_steps = 0;
@@ -520,12 +540,14 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
         if (want && (__popc(want) >= SKG_REFILL_LANES || want == live)) {
             const int leader = __ffs(want) - 1;
             unsigned base = 0;
-            if (lane == leader) base = atomicAdd(W.jcount + 2, (unsigned)__popc(want));
+            if (lane == leader) base = atomicAdd(taken, (unsigned)__popc(want));
             base = __shfl_sync(live, base, leader);
             if (need) {
                 const unsigned jj = base + __popc(want & ((1u << lane) - 1));
                 if (jj >= njobs) break;
-                j = jj < nmainj ? (int)jj : W.npool + (int)(jj - nmainj);
+                if (MODE == 0) j = jj < nmainj ? (int)jj : W.npool + (int)(jj - nmainj);
+                else if (MODE == 1) j = (int)jj;
+                else j = W.npool + (int)jj;
                 const int2 jb = W.jobs[j];
                 p = jb.x;
                 const Packet& K = W.pk[p];
@@ -535,7 +557,7 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
                 const int hint = K.pos_cell;
                 kext1 = (S.ncomp == 1) ? (float)S.kext[ell] : -1.f;
                 R kx, ky, kz;
-                if (jb.y == JOB_MAIN) { kx = (R)K.kx; ky = (R)K.ky; kz = (R)K.kz; kind = 1; v1 = K.L; v2 = 0; }
+                if (MODE != 2 && jb.y == JOB_MAIN) { kx = (R)K.kx; ky = (R)K.ky; kz = (R)K.kz; kind = 1; v1 = K.L; v2 = 0; }
                 else { kx = (R)S.gkx[jb.y]; ky = (R)S.gky[jb.y]; kz = (R)S.gkz[jb.y]; kind = 0; }
                 st.init(sg[slot], (R)K.x, (R)K.y, (R)K.z, kx, ky, kz, hint);
                 if (kind == 1 && hint == -2) W.pk[p].pos_cell = st.cell0;
@@ -563,7 +585,9 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
                     const bool store = (phase == SKG_PHASE_STELLAR) ? (S.store_abs != 0) : (phase == SKG_PHASE_DUST_SELFABS);
                     if (S.ncomp == 1) {
                         if (store) {
-                            const double Lintm = v1 * exp(-tau) * (-expm1(-dtau));
+                            const double em = expm1(-dtau);
+                            const double Lintm = -v1 * em;          // L e^-tau (1 - e^-dtau)
+                            v1 += v1 * em;
                             double* labs = (phase == SKG_PHASE_STELLAR) ? S.labs_stel : S.labs_dust;
                             atomicAdd(labs + (size_t)m * S.nlambda + ell, (1.0 - S.albedo[ell]) * Lintm);
                             atomicAdd(&s_cnt[C_ABS], 1ull);
@@ -575,7 +599,9 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
                             ksca += rh * S.ksca[h * S.nlambda + ell]; kext += rh * S.kext[h * S.nlambda + ell];
                         }
                         const double alb = (kext > 0.0) ? ksca / kext : 0.0;
-                        const double Lintm = v1 * exp(-tau) * (-expm1(-dtau));
+                        const double em = expm1(-dtau);
+                        const double Lintm = -v1 * em;
+                        v1 += v1 * em;
                         v2 += alb * Lintm;
                         if (store) {
                             double* labs = (phase == SKG_PHASE_STELLAR) ? S.labs_stel : S.labs_dust;
@@ -610,7 +636,7 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
                 W.jtau[j] = tau;
                 j = -1;
             } else if (kind == 1) {
-                double L = v1, tau_int = 0;
+                double L = W.pk[p].L, tau_int = 0;     // the packet's luminosity at the path start
                 const int rc = after_path(W, S, p, phase, ell, tau, v2, L, tau_int);
                 if (rc == 1) {
                     const Packet& K = W.pk[p];
@@ -641,24 +667,32 @@ __global__ void __launch_bounds__(256, SKG_TRAV_MIN_BLOCKS) trav_kernel(const Wa
 
 namespace {
 
+// Resident blocks of a traversal instantiation (persistent grid = this many blocks per SM x SMs).
+template<typename R, template<typename> class Stepper, int MODE>
+int resident_blocks(size_t smem) {
+    static int per = 0, sms = 0;
+    if (per == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trav_kernel<R, Stepper, MODE>, 256, smem);
+        if (per <= 0) per = 1;
+    }
+    return sms * per;
+}
+
 template<typename R, template<typename> class Stepper>
 cudaError_t enqueue_wave(const WaveParams& W, int nslots, int trav_blocks, cudaEvent_t mid, cudaStream_t s) {
-    auto trav = trav_kernel<R, Stepper>;
     const size_t smem = (size_t)nslots * sizeof(DevGrid);
-    if (trav_blocks <= 0) {
-        static int per = 0, sms = 0;              // resident blocks of this instantiation
-        if (per == 0) {
-            int dev = 0;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trav, 256, smem);
-            if (per <= 0) per = 1;
-        }
-        trav_blocks = sms * per;
-    }
     event_kernel<R><<<(W.npool + 255) / 256, 256, 0, s>>>(W);
     if (mid) cudaEventRecord(mid, s);
-    trav<<<trav_blocks, 256, smem, s>>>(W);
+#if SKG_SPLIT_TRAV
+    // the path jobs, then the peel-off jobs in their lean kernel
+    trav_kernel<R, Stepper, 1><<<trav_blocks > 0 ? trav_blocks : resident_blocks<R, Stepper, 1>(smem), 256, smem, s>>>(W);
+    trav_kernel<R, Stepper, 2><<<resident_blocks<R, Stepper, 2>(smem), 256, smem, s>>>(W);
+#else
+    trav_kernel<R, Stepper, 0><<<trav_blocks > 0 ? trav_blocks : resident_blocks<R, Stepper, 0>(smem), 256, smem, s>>>(W);
+#endif
     return cudaGetLastError();
 }
 
@@ -727,10 +761,10 @@ cudaError_t WaveRunner::enqueue(int n) {
         const int w = waves_ + i, b = w & 1;
         WaveParams W;
         W.R = P_; W.pk = pk_; W.npool = npool_; W.wave = w;
-        W.jobs = jobs_[b]; W.jtau = jtau_[b]; W.jL = jL_[b]; W.jcount = ctr_ + 4 * b;
+        W.jobs = jobs_[b]; W.jtau = jtau_[b]; W.jL = jL_[b]; W.jcount = ctr_ + 8 * b;
         W.pjobs = jobs_[b ^ 1]; W.pjtau = jtau_[b ^ 1]; W.pjL = jL_[b ^ 1];
-        W.last_busy = ctr_ + 8;
-        if ((e = cudaMemsetAsync(ctr_ + 4 * b, 0, 4 * sizeof(unsigned), stream_)) != cudaSuccess) return e;
+        W.last_busy = ctr_ + 16;
+        if ((e = cudaMemsetAsync(ctr_ + 8 * b, 0, 8 * sizeof(unsigned), stream_)) != cudaSuccess) return e;
         if (timed_) {
             while (ev_.size() < 3 * (size_t)(w + 1)) {
                 cudaEvent_t x;
@@ -782,10 +816,10 @@ cudaError_t WaveRunner::finish(int timeout_ms, cudaEvent_t end, bool* timed_out)
             }
             std::this_thread::sleep_for(std::chrono::microseconds(50));
         }
-        const unsigned busy = h_ctr_[4 * ((waves_ - 1) & 1) + 3];
+        const unsigned busy = h_ctr_[8 * ((waves_ - 1) & 1) + 3];
         if (busy == 0) {
             pending_ = false;
-            estimate = (int)h_ctr_[8] + 3;        // the last busy wave, the detection wave, one spare
+            estimate = (int)h_ctr_[16] + 3;        // the last busy wave, the detection wave, one spare
             break;
         }
         cudaError_t e = enqueue(estimate > 32 ? estimate / 4 : 8);

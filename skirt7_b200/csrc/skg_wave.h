@@ -52,8 +52,8 @@ private:
     double* jtau_[2] = {nullptr, nullptr};
     double* jL_[2] = {nullptr, nullptr};
     size_t cap_jobs_ = 0;
-    static constexpr int NCTR = 9;
-    unsigned* ctr_ = nullptr;         // [4b .. 4b+3]: counters of job buffer b; [8]: last busy wave
+    static constexpr int NCTR = 17;
+    unsigned* ctr_ = nullptr;         // [8b .. 8b+7]: counters of job buffer b; [16]: last busy wave
     unsigned* h_ctr_ = nullptr;       // pinned copy read by finish()
     cudaEvent_t copied_ = nullptr;
 
