@@ -51,11 +51,21 @@ namespace skg {
 #ifndef SKG_SPLIT_TRAV
 #define SKG_SPLIT_TRAV 1
 #endif
+// programmatic dependent launch of the peel-off-job kernel after the path-job kernel
+#ifndef SKG_PDL
+#define SKG_PDL 1
+#endif
 // the event pass at 4 blocks of 256 per SM (64 registers, spilling part of the packet record):
 // its divergent, latency-bound code gains more from the warps than it loses to the spills
 // (octree disk, 10^7 packets: 34.6 ms against 45.2 ms at 2 blocks and 126 registers)
 #ifndef SKG_EVENT_MIN_BLOCKS
 #define SKG_EVENT_MIN_BLOCKS 4
+#endif
+// threads per event-pass block: a block's slot on an SM is held until its slowest record is done,
+// so small blocks free slots sooner (octree disk, 10^7 packets: event pass 29.5 ms with 64 threads,
+// 32.4 with 128, 34.6 with 256)
+#ifndef SKG_EVENT_THREADS
+#define SKG_EVENT_THREADS 64
 #endif
 // a lane whose job ended takes the next one when this many lanes of its warp (or all of its live
 // lanes) wait for one: the job start (job, packet record, start leaf: dependent loads) is then paid
@@ -297,7 +307,7 @@ SKG_D int peel_jobs(const DevScene& S, int ell, bool scat, int cell, double kx, 
 constexpr int SED_PRIV = 1024;          // SED bins a block keeps privately (8 KB)
 
 template<typename R>
-__global__ void __launch_bounds__(256, SKG_EVENT_MIN_BLOCKS) event_kernel(const WaveParams W) {
+__global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 / SKG_EVENT_THREADS) event_kernel(const WaveParams W) {
     __shared__ unsigned long long s_cnt[C_N];
     __shared__ double s_sed[SED_PRIV];
     const RunParams& P = W.R;
@@ -513,6 +523,14 @@ __global__ void __launch_bounds__(256, TravBlocks<MODE>::value) trav_kernel(cons
     for (int i = threadIdx.x; i < C_N; i += blockDim.x) s_cnt[i] = 0;
     for (int i = threadIdx.x; i < H.nslots; i += blockDim.x) { sg[i] = P.grids[i]; s_scene[i] = P.scenes[i]; }
     __syncthreads();
+#if SKG_PDL
+    // the path-job kernel lets the peel-off-job kernel of the same wave be scheduled now: its blocks
+    // become resident as this kernel's blocks run out of jobs and exit, so the two overlap in the
+    // tail of this one.  The peel-off kernel reads only what the event pass wrote (complete before
+    // this kernel started); the one word both may touch, a packet's start cell, is written here
+    // only from "unknown" to the cell, and either value is a valid hint for the peel-off walk.
+    if (MODE == 1) asm volatile("griddepcontrol.launch_dependents;");
+#endif
     const unsigned nmainj = W.jcount[0];
     const unsigned njobs = MODE == 0 ? nmainj + W.jcount[1] : MODE == 1 ? nmainj : W.jcount[1];
     unsigned* const taken = W.jcount + (MODE == 2 ? 4 : 2);
@@ -660,6 +678,11 @@ __global__ void __launch_bounds__(256, TravBlocks<MODE>::value) trav_kernel(cons
     atomicAdd(&s_cnt[C_STEPS], (unsigned long long)c_steps);
     __syncthreads();
     if (threadIdx.x < C_N && s_cnt[threadIdx.x]) atomicAdd(P.counters + threadIdx.x, s_cnt[threadIdx.x]);
+#if SKG_PDL
+    // the peel-off kernel completes only after the path-job kernel it overlapped (and its writes
+    // are visible), so the next wave's event pass, ordered after this kernel, sees both
+    if (MODE == 2) asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -684,12 +707,27 @@ int resident_blocks(size_t smem) {
 template<typename R, template<typename> class Stepper>
 cudaError_t enqueue_wave(const WaveParams& W, int nslots, int trav_blocks, cudaEvent_t mid, cudaStream_t s) {
     const size_t smem = (size_t)nslots * sizeof(DevGrid);
-    event_kernel<R><<<(W.npool + 255) / 256, 256, 0, s>>>(W);
+    event_kernel<R><<<(W.npool + SKG_EVENT_THREADS - 1) / SKG_EVENT_THREADS, SKG_EVENT_THREADS, 0, s>>>(W);
     if (mid) cudaEventRecord(mid, s);
 #if SKG_SPLIT_TRAV
     // the path jobs, then the peel-off jobs in their lean kernel
     trav_kernel<R, Stepper, 1><<<trav_blocks > 0 ? trav_blocks : resident_blocks<R, Stepper, 1>(smem), 256, smem, s>>>(W);
+#if SKG_PDL
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(resident_blocks<R, Stepper, 2>(smem));
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, trav_kernel<R, Stepper, 2>, W);
+    if (e != cudaSuccess) return e;
+#else
     trav_kernel<R, Stepper, 2><<<resident_blocks<R, Stepper, 2>(smem), 256, smem, s>>>(W);
+#endif
 #else
     trav_kernel<R, Stepper, 0><<<trav_blocks > 0 ? trav_blocks : resident_blocks<R, Stepper, 0>(smem), 256, smem, s>>>(W);
 #endif

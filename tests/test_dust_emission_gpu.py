@@ -45,14 +45,19 @@ def gpu_run(m, npp, seed):
 
 def test_dust_emission_matches_oracle(orc):
     m = pan_model()
-    G = [gpu_run(m, 40000, 100 + 10 * b) for b in range(12)]
+    # Both sides run the same packets per wavelength: the temperatures, hence the dust emission,
+    # are a nonlinear function of the noisy absorbed luminosities, so batches of different sizes
+    # have different expectations (with 10x more packets on one side the 1-14 micron dust
+    # self-absorption differed by up to 90 % and the mean cell temperature by 1.3 %; with equal
+    # sizes they agree to 0.1 %).
+    G = [gpu_run(m, 4000, 100 + 10 * b) for b in range(24)]
     O = []
     for b in range(12):
         r = orc.simulate(m, 4000, nthreads=8, seed=500 + b, selfabs_cycles=1, dust_emission_phase=True)
         O.append(dict(cube=r["cubes"][0][0], ls=r["labs_stel"], ld=r["labs_dust"], T=r["T"]))
     assert all(g["c"]["errors"] == 0 for g in G)
     # stellar absorption per wavelength (summed over cells) and dust self-absorption.  The standard
-    # errors come from 12 batches a side (about 15 degrees of freedom, heavier tails than a normal
+    # errors come from 24 and 12 batches (about 20 degrees of freedom, heavier tails than a normal
     # z), and the oracle batches carry a few percent of noise each: bound the largest of the 16
     # |z| by 5 and their median by 1.5
     z, ok = zscores([g["ls"].sum(0) for g in G], [o["ls"].sum(0) for o in O])
