@@ -45,6 +45,12 @@ namespace skg {
 // that holds the optical depth alone (no spills at 64 registers).  Octree disk, 10^7 packets:
 // 202.5 ms against 214.2 ms for one kernel over both (Voronoi disk: 1357 against 1421 ms); the
 // peel-off kernel at 5 or 6 blocks per SM (48 or 40 registers, spilling) is slower (219, 240 ms).
+#ifndef SKG_PATH_MIN_BLOCKS
+#define SKG_PATH_MIN_BLOCKS 4
+#endif
+#ifndef SKG_VOR_PATH_MIN_BLOCKS
+#define SKG_VOR_PATH_MIN_BLOCKS 3
+#endif
 #ifndef SKG_PEEL_MIN_BLOCKS
 #define SKG_PEEL_MIN_BLOCKS 4
 #endif
@@ -509,11 +515,16 @@ SKG_D int after_path(const WaveParams& W, const DevScene& S, int p, int phase, i
 
 // MODE: 0 every job of the wave; 1 the path jobs only; 2 the peel-off jobs only (a lean
 // instantiation: optical depth alone, no path state)
-template<int MODE> struct TravBlocks { static constexpr int value = SKG_TRAV_MIN_BLOCKS; };
-template<> struct TravBlocks<2> { static constexpr int value = SKG_PEEL_MIN_BLOCKS; };
+// Resident blocks per SM of each instantiation.  The Voronoi path-job kernel runs at 3 blocks (80
+// registers, no spills: its neighbour scan keeps more state): 1219 against 1273 ms per 10^7-packet
+// phase; the tree and Cartesian ones are faster at 4 (189 against 194 ms, 94 against 100 ms).
+template<int MODE, template<typename> class Stepper> struct TravBlocks { static constexpr int value = SKG_TRAV_MIN_BLOCKS; };
+template<template<typename> class Stepper> struct TravBlocks<1, Stepper> { static constexpr int value = SKG_PATH_MIN_BLOCKS; };
+template<> struct TravBlocks<1, VoronoiStepper> { static constexpr int value = SKG_VOR_PATH_MIN_BLOCKS; };
+template<template<typename> class Stepper> struct TravBlocks<2, Stepper> { static constexpr int value = SKG_PEEL_MIN_BLOCKS; };
 
 template<typename R, template<typename> class Stepper, int MODE>
-__global__ void __launch_bounds__(256, TravBlocks<MODE>::value) trav_kernel(const WaveParams W) {
+__global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_kernel(const WaveParams W) {
     extern __shared__ unsigned char smem_raw[];
     DevGrid* sg = reinterpret_cast<DevGrid*>(smem_raw);
     __shared__ const DevScene* s_scene[MAX_SLOTS];
