@@ -34,6 +34,7 @@
 #include "skg_wave.h"
 
 #include <chrono>
+#include <cstdlib>
 #include <thread>
 
 namespace skg {
@@ -477,6 +478,38 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 
 // ---------------------------------------------------------------------------------------------
 // traversal pass
 
+// Absorption in cell m of a path step: simulateescapeandabsorption (MonteCarloSimulation.cpp:441-462)
+// with OligoDustSystem::absorb / PanDustSystem::absorb.  v1 = L e^-tau on entry (a running product,
+// one expm1 per absorbing step: L e^-tau (1 - e^-dtau) = -v1 expm1(-dtau)); v2 accumulates L_sca with
+// the local albedo when there are several dust components.  Returns 1 when a tally was stored.
+template<typename R>
+SKG_D int absorb_step(const DevScene& S, int phase, int m, int ell, double dtau, double& v1, double& v2) {
+    if (m < 0) return 0;
+    const bool store = (phase == SKG_PHASE_STELLAR) ? (S.store_abs != 0) : (phase == SKG_PHASE_DUST_SELFABS);
+    double* labs = (phase == SKG_PHASE_STELLAR) ? S.labs_stel : S.labs_dust;
+    if (S.ncomp == 1) {
+        if (!store) return 0;
+        const double em = expm1(-dtau);
+        const double Lintm = -v1 * em;
+        v1 += v1 * em;
+        atomicAdd(labs + (size_t)m * S.nlambda + ell, (1.0 - S.albedo[ell]) * Lintm);
+        return 1;
+    }
+    double ksca = 0, kext = 0;
+    for (int h = 0; h < S.ncomp; h++) {
+        const double rh = rho_load<R>(S, (size_t)h * S.ncells + m);
+        ksca += rh * S.ksca[h * S.nlambda + ell]; kext += rh * S.kext[h * S.nlambda + ell];
+    }
+    const double alb = (kext > 0.0) ? ksca / kext : 0.0;
+    const double em = expm1(-dtau);
+    const double Lintm = -v1 * em;
+    v1 += v1 * em;
+    v2 += alb * Lintm;
+    if (!store) return 0;
+    atomicAdd(labs + (size_t)m * S.nlambda + ell, (1.0 - alb) * Lintm);
+    return 1;
+}
+
 // End of the packet's own path (simulateescapeandabsorption :441-462, the termination test of
 // dostellaremissionchunk :283, simulatepropagation :513-531).  Returns 1 when the path must be
 // re-walked to tau_int (the packet's luminosity is then already in its record), 0 when the packet
@@ -610,35 +643,7 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
             if (kind == 0) {
                 tau += dtau;
             } else if (kind == 1) {
-                if (m >= 0) {
-                    const bool store = (phase == SKG_PHASE_STELLAR) ? (S.store_abs != 0) : (phase == SKG_PHASE_DUST_SELFABS);
-                    if (S.ncomp == 1) {
-                        if (store) {
-                            const double em = expm1(-dtau);
-                            const double Lintm = -v1 * em;          // L e^-tau (1 - e^-dtau)
-                            v1 += v1 * em;
-                            double* labs = (phase == SKG_PHASE_STELLAR) ? S.labs_stel : S.labs_dust;
-                            atomicAdd(labs + (size_t)m * S.nlambda + ell, (1.0 - S.albedo[ell]) * Lintm);
-                            atomicAdd(&s_cnt[C_ABS], 1ull);
-                        }
-                    } else {
-                        double ksca = 0, kext = 0;
-                        for (int h = 0; h < S.ncomp; h++) {
-                            const double rh = rho_load<R>(S, (size_t)h * S.ncells + m);
-                            ksca += rh * S.ksca[h * S.nlambda + ell]; kext += rh * S.kext[h * S.nlambda + ell];
-                        }
-                        const double alb = (kext > 0.0) ? ksca / kext : 0.0;
-                        const double em = expm1(-dtau);
-                        const double Lintm = -v1 * em;
-                        v1 += v1 * em;
-                        v2 += alb * Lintm;
-                        if (store) {
-                            double* labs = (phase == SKG_PHASE_STELLAR) ? S.labs_stel : S.labs_dust;
-                            atomicAdd(labs + (size_t)m * S.nlambda + ell, (1.0 - alb) * Lintm);
-                            atomicAdd(&s_cnt[C_ABS], 1ull);
-                        }
-                    }
-                }
+                if (absorb_step<R>(S, phase, m, ell, dtau, v1, v2)) atomicAdd(&s_cnt[C_ABS], 1ull);
                 tau += dtau;
             } else {
                 const double tn = tau + dtau, sn = v1 + (double)ds;
@@ -697,6 +702,194 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
 }
 
 // ---------------------------------------------------------------------------------------------
+// tail pass: the end of a phase
+//
+// When few packets are left in flight, each wave costs about as long as its longest walk while
+// most of the device idles, and a packet still needs a wave per event.  The tail pass gives every
+// remaining packet a thread that runs the rest of its life at once -- the previous wave's pending
+// peel-off detections, then interaction, scattering peel-offs, scattering, path and re-walk until
+// it terminates, then further packets while the work counter has any -- with the same random
+// streams, samplers and tallies as the waves (device functions shared with the event and traversal
+// passes), so a phase gives the same results with or without it, up to the summation order of the
+// FP64 tally atomics.
+
+// Optical depth from (x, y, z) toward (kx, ky, kz) to the edge of the grid (DustSystem::opticaldepth,
+// DustSystem.cpp:960-976).
+template<typename R, template<typename> class Stepper>
+SKG_D double tail_tau(const DevGrid& g, const DevScene& S, int ell, R x, R y, R z, R kx, R ky, R kz, int hint,
+                      unsigned long long* cnt, unsigned* err) {
+    Stepper<R> st;
+    st.init(g, x, y, z, kx, ky, kz, hint);
+    const float kext1 = (S.ncomp == 1) ? (float)S.kext[ell] : -1.f;
+    double tau = 0;
+    int m; R ds;
+    while (st.walk(g, m, ds)) {
+        cnt[C_STEPS]++;
+        const double kr = (kext1 >= 0.f && st.rho >= 0.f) ? (double)(kext1 * st.rho) : kappa_rho<R>(S, m, ell);
+        tau += kr * (double)ds;
+    }
+    cnt[C_TRAV]++; cnt[C_NBR] += st.nscanned(); cnt[C_FB] += st.fallbacks;
+    if (st.steps > g.max_steps) { atomicOr(err, ERR_STEP_BUDGET); cnt[C_ERR]++; }
+    return tau;
+}
+
+// The peel-offs of the packet from its position (peeloffemission :299-309, peeloffscattering
+// :313-357): one traversal per direction group that needs one, detected at once.  nsp: the
+// scattering count the peel-off copy carries (0 for emission).
+template<typename R, template<typename> class Stepper>
+SKG_D void tail_peel(const DevGrid& g, const DevScene& S, const Packet& K, bool scat, int nsp, double kx0,
+                     double ky0, double kz0, unsigned long long* cnt, unsigned* err) {
+    for (int grp = 0; grp < S.ngroups; grp++) {
+        double w = 1.0;
+        if (scat) {
+            w = peel_weight(S, K.ell, K.int_cell, kx0, ky0, kz0, S.gkx[grp], S.gky[grp], S.gkz[grp]);
+            if (w < 0) break;
+        }
+        if (!group_needs_traversal(S, grp, K.x, K.y, K.z)) continue;
+        const double tau = tail_tau<R, Stepper>(g, S, K.ell, (R)K.x, (R)K.y, (R)K.z, (R)S.gkx[grp], (R)S.gky[grp],
+                                                (R)S.gkz[grp], K.pos_cell, cnt, err);
+        cnt[C_PEEL]++;
+        cnt[C_PIX] += detect_group(S, grp, K.ell, K.L * w, tau, nsp, (K.flags & 1) != 0, K.x, K.y, K.z, nullptr);
+    }
+}
+
+// The packet's own path and, when it interacts, the re-walk to the interaction point: the path job
+// of the traversal pass.  Leaves the record in PK_INTERACT or PK_TERM.
+template<typename R, template<typename> class Stepper>
+SKG_D void tail_path(const WaveParams& W, const DevGrid& g, const DevScene& S, int p, int phase,
+                     unsigned long long* cnt) {
+    Packet& K = W.pk[p];
+    const int ell = K.ell;
+    const float kext1 = (S.ncomp == 1) ? (float)S.kext[ell] : -1.f;
+    Stepper<R> st;
+    const int hint = K.pos_cell;
+    st.init(g, (R)K.x, (R)K.y, (R)K.z, (R)K.kx, (R)K.ky, (R)K.kz, hint);
+    if (hint == -2) K.pos_cell = st.cell0;
+    double tau = 0, v1 = K.L, v2 = 0;
+    int m; R ds;
+    while (st.walk(g, m, ds)) {
+        cnt[C_STEPS]++;
+        const double kr = (kext1 >= 0.f && st.rho >= 0.f) ? (double)(kext1 * st.rho) : kappa_rho<R>(S, m, ell);
+        const double dtau = kr * (double)ds;
+        cnt[C_ABS] += absorb_step<R>(S, phase, m, ell, dtau, v1, v2);
+        tau += dtau;
+    }
+    cnt[C_TRAV]++; cnt[C_NBR] += st.nscanned(); cnt[C_FB] += st.fallbacks;
+    if (st.steps > g.max_steps) { atomicOr(W.R.err, ERR_STEP_BUDGET); cnt[C_ERR]++; }
+    double L = K.L, tau_int = 0;
+    const int rc = after_path(W, S, p, phase, ell, tau, v2, L, tau_int);
+    if (rc < 0) cnt[C_ERR]++;
+    if (rc != 1) return;
+    // DustGridPath::pathlength on the re-walked path
+    st.init(g, (R)K.x, (R)K.y, (R)K.z, (R)K.kx, (R)K.ky, (R)K.kz, K.pos_cell);
+    double s = 0;
+    R d0;
+    while (st.pd.pop(d0)) s += (double)d0;
+    tau = 0;
+    while (st.walk(g, m, ds)) {
+        cnt[C_STEPS]++;
+        const double kr = (kext1 >= 0.f && st.rho >= 0.f) ? (double)(kext1 * st.rho) : kappa_rho<R>(S, m, ell);
+        const double tn = tau + kr * (double)ds, sn = s + (double)ds;
+        if (tn > tau_int) {
+            K.s_int = s + ((tau_int - tau) / (tn - tau)) * (sn - s);
+            K.int_cell = m;
+            K.state = PK_INTERACT;
+            cnt[C_TRAV]++; cnt[C_NBR] += st.nscanned(); cnt[C_FB] += st.fallbacks;
+            return;
+        }
+        tau = tn; s = sn;
+    }
+    cnt[C_TRAV]++; cnt[C_NBR] += st.nscanned(); cnt[C_FB] += st.fallbacks;
+    if (st.steps > g.max_steps) { atomicOr(W.R.err, ERR_STEP_BUDGET); cnt[C_ERR]++; }
+    K.s_int = s; K.int_cell = -1; K.state = PK_INTERACT;
+}
+
+template<typename R, template<typename> class Stepper>
+__global__ void __launch_bounds__(128) tail_kernel(const WaveParams W) {
+    const RunParams& P = W.R;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= W.npool) return;
+    Packet& K = W.pk[p];
+    int state = K.state;
+    if (state == PK_DONE) return;
+    const BatchHeader H = *P.hdr;
+    const int phase = H.phase;
+    const bool peel_on = phase != SKG_PHASE_DUST_SELFABS;
+    unsigned long long cnt[C_N];
+    for (int c = 0; c < C_N; c++) cnt[c] = 0;
+    if (state == PK_WAIT) {                       // a path job that was not walked (as the event pass)
+        atomicOr(P.err, ERR_CAPACITY); cnt[C_ERR]++; state = PK_TERM;
+    }
+    // the peel-offs walked in the last wave
+    if (K.peel_n > 0) {
+        const DevScene& S = *P.scenes[P.items[K.item].slot];
+        const int nsp = (K.flags & 2) ? K.nscatt : 0;
+        for (int i = 0; i < K.peel_n; i++) {
+            const int j = K.peel_j0 + i;
+            cnt[C_PIX] += detect_group(S, W.pjobs[j].y, K.ell, W.pjL[j], W.pjtau[j], nsp, (K.flags & 1) != 0,
+                                       K.x, K.y, K.z, nullptr);
+        }
+        cnt[C_PEEL] += K.peel_n;
+        K.peel_n = 0;
+    }
+    while (true) {
+        if (state == PK_INTERACT) {
+            const WorkItem& It = P.items[K.item];
+            const DevScene& S = *P.scenes[It.slot];
+            const DevGrid& g = P.grids[It.slot];
+            const R si = (R)K.s_int;                // PhotonPackage::propagate
+            K.x = (double)((R)K.x + si * (R)K.kx);
+            K.y = (double)((R)K.y + si * (R)K.ky);
+            K.z = (double)((R)K.z + si * (R)K.kz);
+            if (K.s_int > 0) K.pos_cell = (K.int_cell >= 0) ? K.int_cell : -2;
+            const double kx0 = K.kx, ky0 = K.ky, kz0 = K.kz;
+            if (peel_on) tail_peel<R, Stepper>(g, S, K, true, K.nscatt + 1, kx0, ky0, kz0, cnt, P.err);
+            Philox rng;
+            rng.init(It.seed, K.id, (uint32_t)K.ell | ((uint32_t)phase << 24));
+            rng.c0 = K.rngc;
+            const V3<double> kn = scatter_direction(S, K.ell, K.int_cell, mk3(K.kx, K.ky, K.kz), rng);
+            K.rngc = rng.c0;
+            K.kx = (double)(R)kn.x; K.ky = (double)(R)kn.y; K.kz = (double)(R)kn.z;
+            K.nscatt++;
+            cnt[C_SCATT]++;
+            state = PK_WAIT;
+        }
+        if (state == PK_WAIT) {
+            const int slot = P.items[K.item].slot;
+            tail_path<R, Stepper>(W, P.grids[slot], *P.scenes[slot], p, phase, cnt);
+            state = K.state;
+            continue;
+        }
+        // a free record takes the next packet while there is one
+        const unsigned long long gp = atomicAdd(P.work, 1ull);
+        if (gp >= H.total) break;
+        const int it = find_item(P.items, H.nitems, gp);
+        const WorkItem It = P.items[it];
+        const uint64_t q = gp - It.begin;
+        const int ei = (int)(q / It.count);
+        const uint64_t ip = It.first + (q - (uint64_t)ei * It.count);
+        const int ell = P.ells[It.ell0 + ei];
+        Philox rng;
+        rng.init(It.seed, ip, (uint32_t)ell | ((uint32_t)phase << 24));
+        cnt[C_PACKETS]++;
+        const DevScene& S = *P.scenes[It.slot];
+        const Launched o = launch_packet(P.grids[It.slot], S, phase, ell, It.npp_total, rng);
+        state = PK_TERM;
+        if (!o.ok) continue;
+        K.x = (double)(R)o.x; K.y = (double)(R)o.y; K.z = (double)(R)o.z;
+        K.kx = (double)(R)o.kx; K.ky = (double)(R)o.ky; K.kz = (double)(R)o.kz;
+        K.L = o.L; K.Lth = o.Lth; K.s_int = 0;
+        K.id = ip; K.item = it; K.ell = ell; K.nscatt = 0;
+        K.pos_cell = -2; K.int_cell = -1; K.rngc = rng.c0;
+        K.flags = o.stellar ? 1 : 0; K.peel_n = 0;
+        if (peel_on) tail_peel<R, Stepper>(P.grids[It.slot], S, K, false, 0, 0, 0, 0, cnt, P.err);
+        state = S.ncomp > 0 ? PK_WAIT : PK_TERM;   // without dust the life cycle ends here
+    }
+    K.state = PK_DONE;
+    for (int c = 0; c < C_N; c++) if (cnt[c]) atomicAdd(P.counters + c, cnt[c]);
+}
+
+// ---------------------------------------------------------------------------------------------
 // host side
 
 namespace {
@@ -745,21 +938,32 @@ cudaError_t enqueue_wave(const WaveParams& W, int nslots, int trav_blocks, cudaE
     return cudaGetLastError();
 }
 
-using WaveFn = cudaError_t (*)(const WaveParams&, int, int, cudaEvent_t, cudaStream_t);
+template<typename R, template<typename> class Stepper>
+cudaError_t enqueue_tail(const WaveParams& W, cudaStream_t s) {
+    tail_kernel<R, Stepper><<<(W.npool + 127) / 128, 128, 0, s>>>(W);
+    return cudaGetLastError();
+}
 
-WaveFn pick(int grid_type, int tree_walk, int precision) {
+using WaveFn = cudaError_t (*)(const WaveParams&, int, int, cudaEvent_t, cudaStream_t);
+using TailFn = cudaError_t (*)(const WaveParams&, cudaStream_t);
+struct PassFns { WaveFn wave; TailFn tail; };
+
+template<typename R, template<typename> class Stepper>
+PassFns fns() { return {enqueue_wave<R, Stepper>, enqueue_tail<R, Stepper>}; }
+
+PassFns pick(int grid_type, int tree_walk, int precision) {
     const bool f64 = precision == SKG_PREC_FP64;
     switch (grid_type) {
     case SKG_GRID_CARTESIAN:
-        return f64 ? enqueue_wave<double, CartStepper> : enqueue_wave<float, CartStepper>;
+        return f64 ? fns<double, CartStepper>() : fns<float, CartStepper>();
     case SKG_GRID_OCTREE:
     case SKG_GRID_BINTREE:
-        if (f64) return enqueue_wave<double, TreeStepper>;
-        if (tree_walk == TW_NODES) return enqueue_wave<float, TreeNodeWalk>;
-        if (tree_walk == TW_LATTICE) return enqueue_wave<float, TreeLatticeStepper>;
-        return enqueue_wave<float, TreeStepper>;
+        if (f64) return fns<double, TreeStepper>();
+        if (tree_walk == TW_NODES) return fns<float, TreeNodeWalk>();
+        if (tree_walk == TW_LATTICE) return fns<float, TreeLatticeStepper>();
+        return fns<float, TreeStepper>();
     default:
-        return f64 ? enqueue_wave<double, VoronoiStepper> : enqueue_wave<float, VoronoiStepper>;
+        return f64 ? fns<double, VoronoiStepper>() : fns<float, VoronoiStepper>();
     }
 }
 
@@ -767,6 +971,7 @@ WaveFn pick(int grid_type, int tree_walk, int precision) {
 
 WaveRunner::~WaveRunner() {
     for (cudaEvent_t e : ev_) cudaEventDestroy(e);
+    for (cudaEvent_t e : tail_ev_) if (e) cudaEventDestroy(e);
     cudaFree(pk_);
     for (int b = 0; b < 2; b++) { cudaFree(jobs_[b]); cudaFree(jtau_[b]); cudaFree(jL_[b]); }
     cudaFree(ctr_);
@@ -804,7 +1009,7 @@ cudaError_t WaveRunner::reserve(size_t pool, int ngroups) {
 }
 
 cudaError_t WaveRunner::enqueue(int n) {
-    WaveFn fn = pick(grid_type_, tree_walk_, precision_);
+    WaveFn fn = pick(grid_type_, tree_walk_, precision_).wave;
     cudaError_t e;
     for (int i = 0; i < n; i++) {
         const int w = waves_ + i, b = w & 1;
@@ -838,7 +1043,9 @@ cudaError_t WaveRunner::begin(const RunParams& P, int grid_type, int tree_walk, 
                               size_t npool, int trav_blocks, cudaStream_t s) {
     if (npool == 0 || npool > cap_pool_) return cudaErrorInvalidValue;
     P_ = P; grid_type_ = grid_type; tree_walk_ = tree_walk; precision_ = precision; nslots_ = nslots;
-    trav_blocks_ = trav_blocks; stream_ = s; npool_ = (int)npool; waves_ = 0;
+    trav_blocks_ = trav_blocks; stream_ = s; npool_ = (int)npool; waves_ = 0; tail_ran_ = false;
+    const char* td = std::getenv("SKG_TAIL_DIV");
+    tail_div_ = td ? std::atoi(td) : tail_div;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(s, &cs);
     timed_ = timing && cs == cudaStreamCaptureStatusNone;
@@ -847,6 +1054,24 @@ cudaError_t WaveRunner::begin(const RunParams& P, int grid_type, int tree_walk, 
     if ((e = cudaMemsetAsync(ctr_, 0, NCTR * sizeof(unsigned), s)) != cudaSuccess) return e;
     pending_ = true;
     return enqueue(estimate);
+}
+
+cudaError_t WaveRunner::enqueue_tail() {
+    const int b = (waves_ - 1) & 1;               // the last wave's jobs hold the pending peel-offs
+    WaveParams W;
+    W.R = P_; W.pk = pk_; W.npool = npool_; W.wave = waves_;
+    W.jobs = nullptr; W.jtau = nullptr; W.jL = nullptr; W.jcount = ctr_ + 8 * (b ^ 1);
+    W.pjobs = jobs_[b]; W.pjtau = jtau_[b]; W.pjL = jL_[b];
+    W.last_busy = ctr_ + 16;
+    cudaError_t e;
+    if (timed_) {
+        for (int i = 0; i < 2; i++)
+            if (!tail_ev_[i] && (e = cudaEventCreate(&tail_ev_[i])) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(tail_ev_[0], stream_)) != cudaSuccess) return e;
+    }
+    if ((e = pick(grid_type_, tree_walk_, precision_).tail(W, stream_)) != cudaSuccess) return e;
+    tail_ran_ = true;
+    return timed_ ? cudaEventRecord(tail_ev_[1], stream_) : cudaSuccess;
 }
 
 cudaError_t WaveRunner::finish(int timeout_ms, cudaEvent_t end, bool* timed_out) {
@@ -871,6 +1096,16 @@ cudaError_t WaveRunner::finish(int timeout_ms, cudaEvent_t end, bool* timed_out)
             estimate = (int)h_ctr_[16] + 3;        // the last busy wave, the detection wave, one spare
             break;
         }
+        if (tail_div_ > 0 && (size_t)busy * (size_t)tail_div_ <= (size_t)npool_) {
+            // few packets left in flight: the tail pass finishes them (and any packets still to
+            // launch) in one launch; the next phase enqueues this many waves before it looks
+            cudaError_t e = enqueue_tail();
+            pending_ = false;
+            if (e != cudaSuccess) return e;
+            estimate = waves_;
+            more = true;
+            break;
+        }
         cudaError_t e = enqueue(estimate > 32 ? estimate / 4 : 8);
         if (e != cudaSuccess) { pending_ = false; return e; }
         more = true;
@@ -887,6 +1122,12 @@ cudaError_t WaveRunner::times(float* event_ms, float* trav_ms) const {
             if (e == cudaSuccess) e = cudaEventElapsedTime(&y, ev_[3 * w + 1], ev_[3 * w + 2]);
             if (e != cudaSuccess) return e;
             a += x; t += y;
+        }
+        if (tail_ran_) {
+            float y = 0;
+            cudaError_t e = cudaEventElapsedTime(&y, tail_ev_[0], tail_ev_[1]);
+            if (e != cudaSuccess) return e;
+            t += y;
         }
     }
     if (event_ms) *event_ms = a;

@@ -5,7 +5,8 @@
 // packets to their interaction point, scatter, and write the next traversals as jobs) followed by
 // a traversal pass that walks every job of the wave.  The number of waves is not known in
 // advance: begin() enqueues an estimate, finish() reads how many packets still had work after the
-// last enqueued wave and enqueues more until none has.
+// last enqueued wave and enqueues more until none has -- or, once few have, the tail pass, which
+// finishes every remaining packet in one launch.
 #pragma once
 #include "skg_scene.cuh"
 
@@ -42,9 +43,13 @@ public:
     cudaError_t times(float* event_ms, float* trav_ms) const;
 
     int estimate = 24;                // waves the next phase enqueues up front
+    // the tail pass takes over when at most npool / tail_div packets had work in the last wave
+    // (0: waves to the end; the environment variable SKG_TAIL_DIV overrides it per phase)
+    int tail_div = 16;
 
 private:
     cudaError_t enqueue(int n);
+    cudaError_t enqueue_tail();
 
     Packet* pk_ = nullptr;
     size_t cap_pool_ = 0;
@@ -66,6 +71,9 @@ private:
     int waves_ = 0;
     std::vector<cudaEvent_t> ev_;      // 3 per wave: before the event pass, between, after the traversal
     bool timed_ = false;               // the running phase records ev_
+    int tail_div_ = 16;
+    bool tail_ran_ = false;            // the phase ended with the tail pass
+    cudaEvent_t tail_ev_[2] = {nullptr, nullptr};
 };
 
 }  // namespace skg

@@ -31,3 +31,37 @@ def test_pool_and_blocks_do_not_change_results():
     assert res["pool"] in (1 << 12, 1 << 14) and res["blocks"] in (148, 296) and len(res["trials"]) == 4
     assert autotune.tune(ctx, A.PHASE_STELLAR, [0], 60000) is res          # cached per workload class
     ctx.close()
+
+
+@pytest.mark.parametrize("grid", ["cartesian", "octree"])
+def test_tail_pass_does_not_change_results(grid, monkeypatch):
+    """The tail pass (one thread per remaining packet runs the rest of its life at once) uses the
+    same random streams, samplers and tallies as the waves: a phase ending in waves only, in the
+    tail pass from the default threshold, or handing nearly all its work to the tail pass (which
+    then launches the remaining packets itself) gives the same frames and absorbed luminosities up
+    to the summation order of the FP64 atomics, and the same counts."""
+    m = models.oligo_disk(N=(40, 40, 20))
+    if grid == "octree":
+        from skirt7_b200.scene import KPC
+        ext = (-20 * KPC, -20 * KPC, -2 * KPC, 20 * KPC, 20 * KPC, 2 * KPC)
+        m.dustGrid = runtime.build_tree(m, A.GRID_OCTREE, ext, minLevel=2, maxLevel=6, maxMassFraction=1e-4)
+        m.rho = None
+    else:
+        m.rho = cell_center_density(m)
+    ctx = runtime.Context(m)
+    res = []
+    for div in ("0", "16", "1"):
+        monkeypatch.setenv("SKG_TAIL_DIV", div)
+        ctx.reset_tallies()
+        ctx.run_phase(A.PHASE_STELLAR, [0], 200000, 0, 200000, seed=7, pool=1 << 16)
+        ctx.sync()
+        c = ctx.counters()
+        res.append((ctx.read_instrument(0)[0].copy(), ctx.read_absorption()[0].copy(), c))
+    f0, l0, c0 = res[0]
+    assert c0["errors"] == 0 and c0["packets"] == 200000
+    for f, l, c in res[1:]:
+        assert np.allclose(f, f0, rtol=1e-10, atol=1e-12 * f0.max())
+        assert np.allclose(l, l0, rtol=1e-10, atol=1e-12 * l0.max())
+        for k in ("packets", "scatterings", "peeloffs", "traversals", "errors"):
+            assert c[k] == c0[k], (k, c[k], c0[k])
+    ctx.close()
