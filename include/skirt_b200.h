@@ -171,6 +171,11 @@ typedef struct skg_instrument {
     int32_t nxp, nyp;                       /* pixels (SingleFrameInstrument) */
     double fovx, fovy, xc, yc;              /* field of view and centre (m) */
     int32_t nscatt_levels;                  /* FullInstrument::_Nscatt */
+    int32_t stellar_comps;                  /* FRAME: also one frame per stellar component, the
+                                               peel-offs of the packets it launched (components
+                                               1..nstellar after the total; the frames FitSKIRT fits,
+                                               MultiFrameInstrument::writeStellarComps,
+                                               MultiFrameInstrument.cpp:17-57) */
 } skg_instrument;
 
 typedef struct skg_scene {

@@ -833,7 +833,7 @@ struct Instrument {
     vector<double> cube, sed;    // [ncomp][nlambda][Nyp][Nxp], [ncomp][nlambda]
     std::mutex* lock = nullptr;
 
-    void setup(const skg_instrument& in, int nlambda) {
+    void setup(const skg_instrument& in, int nlambda, int nstellar) {
         type = in.type;
         costheta = std::cos(in.inclination); sintheta = std::sin(in.inclination);
         cosphi = std::cos(in.azimuth); sinphi = std::sin(in.azimuth);
@@ -845,6 +845,7 @@ struct Instrument {
             ypmin = in.yc - 0.5*in.fovy; ypsiz = in.fovy/Nyp;
         }
         if (type == SKG_INSTR_FULL) { nscatt_levels = in.nscatt_levels; ncomp = SKG_FULL_NBASE + nscatt_levels; }
+        if (type == SKG_INSTR_FRAME && in.stellar_comps) ncomp = 1 + nstellar;   // MultiFrameInstrument.cpp:17-57
         if (type != SKG_INSTR_SED) cube.assign((size_t)ncomp*nlambda*Nxp*Nyp, 0.0);
         sed.assign((size_t)ncomp*nlambda, 0.0);
     }
@@ -925,7 +926,11 @@ static void detect(Sim& S, Instrument& I, const Packet& pp, Path& path) {
         int l = I.pixel(pp.r);
         if (l >= 0) {
             double taupath = S.opticaldepth(path, pp.ell);
-            atomic_add(I.cube[(size_t)pp.ell*I.Nxp*I.Nyp + l], pp.L*std::exp(-taupath));
+            const size_t fp = (size_t)I.Nxp*I.Nyp;
+            atomic_add(I.cube[(size_t)pp.ell*fp + l], pp.L*std::exp(-taupath));
+            // the frame of the packet's stellar component (writeStellarComps)
+            if (I.ncomp > 1 && pp.stellar >= 0)
+                atomic_add(I.cube[((size_t)(1 + pp.stellar)*nl + pp.ell)*fp + l], pp.L*std::exp(-taupath));
         }
         return;
     }
@@ -1267,7 +1272,7 @@ static Sim* buildSim(const skg_scene* sc) {
         if (Nst) cdf(S->Xvv[ell], pv);
     }
     S->instr.resize(sc->ninstr);
-    for (int i = 0; i < sc->ninstr; i++) S->instr[i].setup(sc->instr[i], sc->nlambda);
+    for (int i = 0; i < sc->ninstr; i++) S->instr[i].setup(sc->instr[i], sc->nlambda, sc->nstellar);
     S->minWeightReduction = sc->min_weight_reduction > 0 ? sc->min_weight_reduction : 1e4;
     S->minfs = sc->min_scatt_events;
     S->xi = sc->scatt_bias;

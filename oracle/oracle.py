@@ -136,6 +136,8 @@ def simulate(model, packages, nthreads=8, seed=4357, selfabs_cycles=0, dust_emis
     cubes, seds = [], []
     for ins in model.instruments:
         nc = 1 if ins.type != 3 else 6 + ins.scatteringLevels
+        if ins.type == 1 and getattr(ins, "writeStellarComps", False):
+            nc = 1 + len(model.stellarComps)
         ncomp.append(nc)
         if ins.type == 0:
             cubes.append(None)

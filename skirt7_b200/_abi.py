@@ -83,6 +83,7 @@ class Instrument(C.Structure):
         ("nxp", C.c_int32), ("nyp", C.c_int32),
         ("fovx", C.c_double), ("fovy", C.c_double), ("xc", C.c_double), ("yc", C.c_double),
         ("nscatt_levels", C.c_int32),
+        ("stellar_comps", C.c_int32),
     ]
 
 

@@ -511,6 +511,7 @@ int skg_ctx_create(const skg_scene* sc, int device, skg_ctx** out) {
             else if (th >= M_PI - 1e-8) { I.kx = 0; I.ky = 0; I.kz = -1; }
             else { I.kx = std::sin(th) * std::cos(ph); I.ky = std::sin(th) * std::sin(ph); I.kz = std::cos(th); }
             I.ncomp = 1;
+            if (in.type == SKG_INSTR_FRAME && in.stellar_comps) I.ncomp = 1 + std::max(sc->nstellar, 0);
             if (in.type == SKG_INSTR_FULL) { REQUIRE(in.nscatt_levels >= 0, "scattering levels must be >= 0"); I.nscatt_levels = in.nscatt_levels; I.ncomp = SKG_FULL_NBASE + in.nscatt_levels; }
             if (in.type != SKG_INSTR_SED) {
                 REQUIRE(in.type == SKG_INSTR_FRAME || in.type == SKG_INSTR_SIMPLE || in.type == SKG_INSTR_FULL, "unknown instrument type");

@@ -103,7 +103,8 @@ template<typename R> SKG_D double kappa_rho(const DevScene& S, int m, int ell) {
 // (every packet of a wavelength adds to the same SED bin: global atomics would serialise on it).
 // Returns the number of tally updates.
 __device__ __noinline__ int detect_group(const DevScene& S, int grp, int ell, double Lpeel, double tau,
-                                         int nscatt_peel, bool stellar, double x, double y, double z, double* psed) {
+                                         int nscatt_peel, bool stellar, int comp, double x, double y, double z,
+                                         double* psed) {
     double Lextf = Lpeel * exp(-tau);
     const int nl = S.nlambda;
     int adds = 0;
@@ -118,7 +119,11 @@ __device__ __noinline__ int detect_group(const DevScene& S, int grp, int ell, do
         int l = (I.type == SKG_INSTR_SED) ? -1 : pixel_on_detector(I, x, y, z);
         size_t fp = (size_t)I.nxp * I.nyp;
         if (I.type == SKG_INSTR_FRAME) {
-            if (l >= 0) { atomicAdd(I.cube + (size_t)ell * fp + l, Lextf); adds++; }
+            if (l >= 0) {
+                atomicAdd(I.cube + (size_t)ell * fp + l, Lextf); adds++;
+                // the frame of the packet's stellar component (component 1 + comp)
+                if (I.ncomp > 1 && comp >= 0) { atomicAdd(I.cube + ((size_t)(1 + comp) * nl + ell) * fp + l, Lextf); adds++; }
+            }
         } else if (I.type == SKG_INSTR_SED) {
             sed_add(0, Lextf);
         } else if (I.type == SKG_INSTR_SIMPLE) {
@@ -144,6 +149,10 @@ __device__ __noinline__ int detect_group(const DevScene& S, int grp, int ell, do
     return adds;
 }
 
+// Packet flags: bit 0 stellar origin, bit 1 the pending peel-offs follow a scattering, bits 8-15
+// the launching stellar component + 1 (0: a dust-emission packet).
+SKG_D int pk_comp(const Packet& K) { return ((K.flags >> 8) & 0xff) - 1; }
+
 // Does the group need a traversal?  Frame-only groups skip it when the packet projects off every
 // frame (FrameInstrument.cpp:36-37).
 SKG_D bool group_needs_traversal(const DevScene& S, int grp, double x, double y, double z) {
@@ -153,7 +162,8 @@ SKG_D bool group_needs_traversal(const DevScene& S, int grp, double x, double y,
     return false;
 }
 
-struct Launched { double x, y, z, kx, ky, kz, L, Lth; int ok; int stellar; };
+struct Launched { double x, y, z, kx, ky, kz, L, Lth; int ok; int stellar; int comp; };
+SKG_D int pk_flags(const Launched& o) { return (o.stellar ? 1 : 0) | ((o.comp + 1) << 8); }
 
 // Packet launch: StellarSystem::launch (StellarSystem.cpp:116-158) with the geometry samplers
 // (GeometricStellarComp.cpp:75-81), or a dust-emission launch from the cell luminosity CDF
@@ -162,6 +172,7 @@ __device__ __noinline__ Launched launch_packet(const DevGrid& g, const DevScene&
                                                uint64_t Npp_total, Philox& rng) {
     Launched o;
     o.ok = 0;
+    o.comp = -1;
     const int nl = S.nlambda;
     V3<double> pos, dir;
     if (phase == SKG_PHASE_STELLAR) {
@@ -181,7 +192,7 @@ __device__ __noinline__ Launched launch_packet(const DevGrid& g, const DevScene&
         }
         pos = geom_position(S.stellar[h], rng);
         dir = iso_direction(rng);
-        o.L = Lw; o.stellar = 1;
+        o.L = Lw; o.stellar = 1; o.comp = h;
     } else {
         double Ltot = S.emit_Ltot[ell];
         if (!(Ltot > 0)) return o;
@@ -346,8 +357,8 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 
         int pix = 0;
         for (int i = 0; i < K.peel_n; i++) {
             const int j = K.peel_j0 + i;
-            pix += detect_group(S, W.pjobs[j].y, K.ell, W.pjL[j], W.pjtau[j], nsp, (K.flags & 1) != 0, K.x, K.y, K.z,
-                                psed);
+            pix += detect_group(S, W.pjobs[j].y, K.ell, W.pjL[j], W.pjtau[j], nsp, (K.flags & 1) != 0,
+                                pk_comp(K), K.x, K.y, K.z, psed);
         }
         atomicAdd(&s_cnt[C_PIX], (unsigned long long)pix);
         atomicAdd(&s_cnt[C_PEEL], (unsigned long long)K.peel_n);
@@ -416,7 +427,7 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 
                     K.L = o.L; K.Lth = o.Lth; K.s_int = 0;
                     K.id = ip; K.item = it; K.ell = ell; K.nscatt = 0;
                     K.pos_cell = -2; K.int_cell = -1; K.rngc = rng.c0;
-                    K.flags = o.stellar ? 1 : 0; K.peel_n = 0;
+                    K.flags = pk_flags(o); K.peel_n = 0;
                     npeel = peel_on ? peel_jobs<false>(S, ell, false, -1, 0, 0, 0, K.x, K.y, K.z, K.L, 0, 0, nullptr,
                                                        nullptr)
                                     : 0;
@@ -457,7 +468,7 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 
     K.peel_n = npeel;
     if (nmain) W.jobs[bm + inm - 1] = make_int2(p, JOB_MAIN);
     if (p < W.npool && was_live) {
-        K.flags = (K.flags & 1) | (scat_peel ? 2 : 0);
+        K.flags = (K.flags & ~2) | (scat_peel ? 2 : 0);
         K.state = state;
         W.pk[p] = K;
     }
@@ -749,7 +760,8 @@ SKG_D void tail_peel(const DevGrid& g, const DevScene& S, const Packet& K, bool 
         const double tau = tail_tau<R, Stepper>(g, S, K.ell, (R)K.x, (R)K.y, (R)K.z, (R)S.gkx[grp], (R)S.gky[grp],
                                                 (R)S.gkz[grp], K.pos_cell, cnt, err);
         cnt[C_PEEL]++;
-        cnt[C_PIX] += detect_group(S, grp, K.ell, K.L * w, tau, nsp, (K.flags & 1) != 0, K.x, K.y, K.z, nullptr);
+        cnt[C_PIX] += detect_group(S, grp, K.ell, K.L * w, tau, nsp, (K.flags & 1) != 0, pk_comp(K), K.x, K.y, K.z,
+                                   nullptr);
     }
 }
 
@@ -827,7 +839,7 @@ __global__ void __launch_bounds__(128) tail_kernel(const WaveParams W) {
         for (int i = 0; i < K.peel_n; i++) {
             const int j = K.peel_j0 + i;
             cnt[C_PIX] += detect_group(S, W.pjobs[j].y, K.ell, W.pjL[j], W.pjtau[j], nsp, (K.flags & 1) != 0,
-                                       K.x, K.y, K.z, nullptr);
+                                       pk_comp(K), K.x, K.y, K.z, nullptr);
         }
         cnt[C_PEEL] += K.peel_n;
         K.peel_n = 0;
@@ -881,7 +893,7 @@ __global__ void __launch_bounds__(128) tail_kernel(const WaveParams W) {
         K.L = o.L; K.Lth = o.Lth; K.s_int = 0;
         K.id = ip; K.item = it; K.ell = ell; K.nscatt = 0;
         K.pos_cell = -2; K.int_cell = -1; K.rngc = rng.c0;
-        K.flags = o.stellar ? 1 : 0; K.peel_n = 0;
+        K.flags = pk_flags(o); K.peel_n = 0;
         if (peel_on) tail_peel<R, Stepper>(P.grids[It.slot], S, K, false, 0, 0, 0, 0, cnt, P.err);
         state = S.ncomp > 0 ? PK_WAIT : PK_TERM;   // without dust the life cycle ends here
     }

@@ -342,6 +342,7 @@ class FrameInstrument:
     instrumentName: str = "frame"
     type: int = A.INSTR_FRAME
     scatteringLevels: int = 0
+    writeStellarComps: bool = False   # FRAME: one more frame per stellar component (MultiFrameInstrument)
 
     def lower(self, I: A.Instrument):
         I.type = self.type
@@ -350,6 +351,7 @@ class FrameInstrument:
         I.nxp, I.nyp = self.pixelsX, self.pixelsY
         I.fovx, I.fovy, I.xc, I.yc = self.fieldOfViewX, self.fieldOfViewY, self.centerX, self.centerY
         I.nscatt_levels = self.scatteringLevels
+        I.stellar_comps = int(bool(self.writeStellarComps) and self.type == A.INSTR_FRAME)
 
 
 def SimpleInstrument(**kw):

@@ -154,3 +154,27 @@ def test_fp32_geometry_total_flux_against_fp64(gtype):
         big = b64 > 1e-3 * b64.sum(axis=(1, 2), keepdims=True)
         assert np.median(np.abs(b32[big] / b64[big] - 1)) < 1e-3
     ctx.close()
+
+
+def test_frames_per_stellar_component(orc):
+    """A frame instrument that also writes one frame per stellar component (the frames FitSKIRT
+    fits, MultiFrameInstrument::writeStellarComps): the component frames add up to the total frame
+    (every stellar packet comes from one component) and each agrees with the oracle's."""
+    m = models.oligo_disk(N=(40, 40, 20), npix=60)
+    fov = 40 * KPC
+    m.instruments = [FrameInstrument(distance=10 * MPC, inclination=80 * DEG, pixelsX=60, pixelsY=60,
+                                     fieldOfViewX=fov, fieldOfViewY=fov, instrumentName="comps",
+                                     writeStellarComps=True)]
+    m.rho = cell_center_density(m)
+    assert len(m.stellarComps) == 2
+    G = gpu_batches(m, 12, 200000, A.PREC_FP32)
+    O = oracle_batches(orc, m, 12, 8000)
+    for g in G:
+        cube = g["inst"][0][0]
+        assert cube.shape[0] == 3
+        assert np.allclose(cube[1] + cube[2], cube[0], rtol=1e-10, atol=1e-12 * cube[0].max())
+        assert cube[1].sum() > 0 and cube[2].sum() > 0
+    for c in (1, 2):
+        fc = lambda r, c=c: block_sum(r["inst"][0][0][c, 0], 6)
+        z, ok = _well_sampled(zscores([fc(g) for g in G], [fc(o) for o in O]), O, fc)
+        _check(z, ok, "stellar component frame %d" % c)
