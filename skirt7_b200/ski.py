@@ -362,6 +362,20 @@ def _instrument(c, it):
     pa = c.d(it, "positionAngle", "posangle", 0)
     if k == "SEDInstrument":
         return SEDInstrument(dist, inc, az, pa, **kw)
+    if k == "MultiFrameInstrument":
+        # one InstrumentFrame per wavelength (MultiFrameInstrument.hpp:25-38, InstrumentFrame.hpp:26-60);
+        # supported when all frames share one geometry, as one frame instrument whose cube holds the
+        # total (writeTotal) and, with writeStellarComps, one frame per stellar component
+        geo = []
+        for f in it.many("frames"):
+            geo.append(dict(pixelsX=c.i(f, "pixelsX", 250), pixelsY=c.i(f, "pixelsY", 250),
+                            fieldOfViewX=c.d(f, "fieldOfViewX", "length"),
+                            fieldOfViewY=c.d(f, "fieldOfViewY", "length"),
+                            centerX=c.d(f, "centerX", "length", 0), centerY=c.d(f, "centerY", "length", 0)))
+        if not geo or any(g != geo[0] for g in geo):
+            raise SkiError("MultiFrameInstrument: frames of different sizes are not supported")
+        return FrameInstrument(distance=dist, inclination=inc, azimuth=az, positionAngle=pa,
+                               writeStellarComps=c.b(it, "writeStellarComps", "no"), **geo[0], **kw)
     frame = dict(distance=dist, inclination=inc, azimuth=az, positionAngle=pa,
                  pixelsX=c.i(it, "pixelsX", 250), pixelsY=c.i(it, "pixelsY", 250),
                  fieldOfViewX=c.d(it, "fieldOfViewX", "length"), fieldOfViewY=c.d(it, "fieldOfViewY", "length"),

@@ -95,3 +95,25 @@ def test_fits_round_trip_and_calibration(tmp_path):
     area = (2 * math.atan(s / (2 * d))) ** 2
     L = sb[0, 1, 1] / ((math.pi / 648000) ** 2) * area * 4 * math.pi * d * d * dlam[0] / lam[0]
     assert L == pytest.approx(1e30, rel=1e-12)
+
+
+def test_multiframe_instrument_for_fitskirt():
+    """MultiFrameInstrument (one InstrumentFrame per wavelength, writeStellarComps for FitSKIRT)
+    maps onto a frame instrument with one frame per stellar component when its frames share one
+    geometry; frames of different sizes are refused by name."""
+    frame = ('<InstrumentFrame fieldOfViewX="40 kpc" pixelsX="64" centerX="0 pc" fieldOfViewY="40 kpc" '
+             'pixelsY="64" centerY="0 pc"/>')
+    multi = ('<MultiFrameInstrument instrumentName="fit" distance="10 Mpc" inclination="85 deg" azimuth="0 deg" '
+             'positionAngle="0 deg" writeTotal="true" writeStellarComps="true"><frames>%s</frames>'
+             '</MultiFrameInstrument>' % frame)
+    xml = open(CFG1).read()
+    i0 = xml.index("<FrameInstrument ")
+    i1 = xml.index("/>", i0) + 2
+    s = ski.load(xml[:i0] + multi + xml[i1:])
+    ins = s.model.instruments[0]
+    assert ins.type == A.INSTR_FRAME and ins.writeStellarComps and ins.pixelsX == 64
+    assert ins.inclination == pytest.approx(85 * np.pi / 180)
+    other = frame.replace('pixelsX="64"', 'pixelsX="32"')
+    bad = multi.replace("</frames>", other + "</frames>")
+    with pytest.raises(ski.SkiError, match="different sizes"):
+        ski.load(xml[:i0] + bad + xml[i1:])
