@@ -81,6 +81,9 @@ namespace skg {
 #ifndef SKG_REFILL_LANES
 #define SKG_REFILL_LANES 8
 #endif
+#ifndef SKG_REFILL_PEEL
+#define SKG_REFILL_PEEL SKG_REFILL_LANES
+#endif
 
 enum Cnt : int { C_PACKETS = 0, C_STEPS, C_TRAV, C_SCATT, C_PEEL, C_ABS, C_PIX, C_NBR, C_FB, C_ERR, C_N };
 
@@ -610,7 +613,7 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
         const unsigned live = __activemask();
         const bool need = j < 0;
         const unsigned want = __ballot_sync(live, need);
-        if (want && (__popc(want) >= SKG_REFILL_LANES || want == live)) {
+        if (want && (__popc(want) >= (MODE == 2 ? SKG_REFILL_PEEL : SKG_REFILL_LANES) || want == live)) {
             const int leader = __ffs(want) - 1;
             unsigned base = 0;
             if (lane == leader) base = atomicAdd(taken, (unsigned)__popc(want));
