@@ -81,6 +81,13 @@ namespace skg {
 #ifndef SKG_REFILL_LANES
 #define SKG_REFILL_LANES 8
 #endif
+// lanes whose path walk ended run the end of the path (escape fraction, termination test, the
+// interaction sampling: long, divergent FP64 code) once this many lanes of the warp wait for it,
+// or no lane is walking.  Per 10^7 packets, traversal pass at 1 / 4 / 8 / 16: octree disk 193 /
+// 176 / 170 / 174 ms; at 1 / 8: Cartesian 95 / 71 ms, k-d tree 224 / 201 ms, Voronoi 1212 / 1186 ms.
+#ifndef SKG_AFTER_LANES
+#define SKG_AFTER_LANES 8
+#endif
 #ifndef SKG_REFILL_PEEL
 #define SKG_REFILL_PEEL SKG_REFILL_LANES
 #endif
@@ -613,7 +620,30 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
         const unsigned live = __activemask();
         const bool need = j < 0;
         const unsigned want = __ballot_sync(live, need);
-        if (want && (__popc(want) >= (MODE == 2 ? SKG_REFILL_PEEL : SKG_REFILL_LANES) || want == live)) {
+        // lanes whose path walk ended (kind 3) run the end of the path together
+        const unsigned pend = (MODE == 2) ? 0u : __ballot_sync(live, kind == 3);
+        const bool idle = (live & ~want & ~pend) == 0;      // no lane of the warp is walking
+        if (pend && (__popc(pend) >= SKG_AFTER_LANES || idle)) {
+            if (kind == 3) {
+                const DevGrid& g = sg[slot];
+                const DevScene& S = *s_scene[slot];
+                double L = W.pk[p].L, tau_int = 0;      // the packet's luminosity at the path start
+                const int rc = after_path(W, S, p, phase, ell, tau, v2, L, tau_int);
+                if (rc == 1) {
+                    const Packet& K = W.pk[p];
+                    st.init(g, (R)K.x, (R)K.y, (R)K.z, (R)K.kx, (R)K.ky, (R)K.kz, K.pos_cell);
+                    tau = 0; v1 = 0; v2 = tau_int; kind = 2;
+                    R d0;
+                    while (st.pd.pop(d0)) v1 += (double)d0;
+                } else {
+                    if (rc < 0) atomicAdd(&s_cnt[C_ERR], 1ull);
+                    j = -1;
+                    kind = 0;
+                }
+            }
+            continue;
+        }
+        if (want && (__popc(want) >= (MODE == 2 ? SKG_REFILL_PEEL : SKG_REFILL_LANES) || (live & ~want & ~pend) == 0)) {
             const int leader = __ffs(want) - 1;
             unsigned base = 0;
             if (lane == leader) base = atomicAdd(taken, (unsigned)__popc(want));
@@ -643,7 +673,7 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
             }
         }
 
-        if (j < 0) continue;            // waiting for enough lanes to refill together
+        if (j < 0 || kind == 3) continue;   // waiting for enough lanes to refill / end paths together
 
         // one cell step
         const DevGrid& g = sg[slot];
@@ -684,18 +714,7 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
                 W.jtau[j] = tau;
                 j = -1;
             } else if (kind == 1) {
-                double L = W.pk[p].L, tau_int = 0;     // the packet's luminosity at the path start
-                const int rc = after_path(W, S, p, phase, ell, tau, v2, L, tau_int);
-                if (rc == 1) {
-                    const Packet& K = W.pk[p];
-                    st.init(g, (R)K.x, (R)K.y, (R)K.z, (R)K.kx, (R)K.ky, (R)K.kz, K.pos_cell);
-                    tau = 0; v1 = 0; v2 = tau_int; kind = 2;
-                    R d0;
-                    while (st.pd.pop(d0)) v1 += (double)d0;
-                } else {
-                    if (rc < 0) atomicAdd(&s_cnt[C_ERR], 1ull);
-                    j = -1;
-                }
+                kind = 3;                       // the end of the path runs with other lanes' (above)
             } else {
                 // DustGridPath::pathlength: an optical depth beyond the last segment gives the full length
                 Packet& K = W.pk[p];
