@@ -186,8 +186,8 @@ class Workload:
     # DRAM bytes per cell step of the traversal pass, measured with ncu
     # (dram__bytes_read.sum + dram__bytes_write.sum summed over every traversal launch of one
     # stellar phase, divided by the phase's cell steps; profiles/traffic_per_step.md), FP32 walk
-    NCU_DRAM_BYTES_PER_STEP = {"octree_pan": 11.37, "cartesian_oligo": 3.40, "voronoi_clumpy": 268.05,
-                               "kdtree_dust": 49.15}
+    NCU_DRAM_BYTES_PER_STEP = {"octree_pan": 11.40, "cartesian_oligo": 3.37, "voronoi_clumpy": 260.6,
+                               "kdtree_dust": 47.9}
 
     def frames(self):
         from skirt7_b200 import _abi as A
