@@ -640,11 +640,20 @@ struct TreeStepper<float> {
 // FP32 walk on the lattice form of the rope tree: the same steps as TreeStepper<float>, with the
 // current leaf's 32-byte record (density, centre codes, packed ropes) in registers and its walls
 // computed from the codes.  A leaf reference is the cell number.
+// reciprocal directions for the exit distances of the lattice walk: the traversal kernels are
+// issue-bound, and three multiplies replace three IEEE divisions per cell step (octree disk,
+// traversal pass 164 against 170 ms per 10^7 packets)
+#ifndef SKG_LAT_RCP
+#define SKG_LAT_RCP 1
+#endif
 template<typename R> struct TreeLatticeStepper : TreeNodeWalk<R> {};
 
 template<>
 struct TreeLatticeStepper<float> {
     float x, y, z, kx, ky, kz;
+#if SKG_LAT_RCP
+    float ux, uy, uz;           // 1/k per axis (0 where |k| <= 1e-15: that axis is never crossed)
+#endif
     uint4 a, b;                 // the current leaf's record
     int leaf;                   // its cell number
     Pend<float> pd;
@@ -686,6 +695,11 @@ struct TreeLatticeStepper<float> {
     SKG_D void init(const DevGrid& g, float rx, float ry, float rz, float dx, float dy, float dz, int hint = -1) {
         kx = dx; ky = dy; kz = dz; pd.clear(); done = false; steps = 0; fallbacks = 0;
         cell0 = -1; rho = -1.f;
+#if SKG_LAT_RCP
+        ux = (fabsf(kx) > 1e-15f) ? 1.f / kx : 0.f;
+        uy = (fabsf(ky) > 1e-15f) ? 1.f / ky : 0.f;
+        uz = (fabsf(kz) > 1e-15f) ? 1.f / kz : 0.f;
+#endif
         if (hint >= 0) {
             leaf = hint;
             load(g, leaf);
@@ -710,9 +724,17 @@ struct TreeLatticeStepper<float> {
             const float xnext = wall(code_x(a), kx >= 0.f, g.lorg[0], g.lunit[0]);
             const float ynext = wall(code_y(a), ky >= 0.f, g.lorg[1], g.lunit[1]);
             const float znext = wall(code_z(a), kz >= 0.f, g.lorg[2], g.lunit[2]);
+#if SKG_LAT_RCP
+            // exit distances with the traversal's reciprocal directions: within an ulp of the
+            // quotients, far inside the 4-ulp nudge past each wall
+            float dsx = (ux != 0.f) ? (xnext - x) * ux : FLT_MAX;
+            float dsy = (uy != 0.f) ? (ynext - y) * uy : FLT_MAX;
+            float dsz = (uz != 0.f) ? (znext - z) * uz : FLT_MAX;
+#else
             float dsx = (fabsf(kx) > 1e-15f) ? (xnext - x) / kx : FLT_MAX;
             float dsy = (fabsf(ky) > 1e-15f) ? (ynext - y) / ky : FLT_MAX;
             float dsz = (fabsf(kz) > 1e-15f) ? (znext - z) / kz : FLT_MAX;
+#endif
             float d; int face;          // exit wall: 0..5 = x-, x+, y-, y+, z-, z+
             if (dsx <= dsy && dsx <= dsz) { d = dsx; face = (kx < 0.f) ? 0 : 1; }
             else if (dsy <= dsx && dsy <= dsz) { d = dsy; face = (ky < 0.f) ? 2 : 3; }

@@ -79,16 +79,24 @@ class Server:
     max_slots    simulations per launch (skg_batch slots)
     tick_packets packets per wavelength a request runs per tick at most; smaller ticks let
                  arrivals join sooner, larger ones amortise the launch
+    policy       "fifo": a tick's packets go to the admitted requests in arrival order until
+                 tick_budget packets (all wavelengths) are given out, so the oldest requests finish
+                 first and the longest wait -- the p99 latency of a loaded loop -- is shortest;
+                 "share": every admitted request runs a slice every tick (processor sharing)
     """
 
     def __init__(self, device=0, hbm_budget=40 << 30, max_slots=64, tick_packets=1 << 20, npix=256,
-                 precision=A.PREC_FP32):
+                 precision=A.PREC_FP32, policy="fifo", tick_budget=6 << 20):
         self.device = device
         self.budget = hbm_budget
         self.max_slots = max_slots
         self.tick_packets = int(tick_packets)
         self.npix = npix
         self.precision = precision
+        if policy not in ("fifo", "share"):
+            raise ValueError("policy is 'fifo' or 'share'")
+        self.policy = policy
+        self.tick_budget = int(tick_budget)
         self.batch = runtime.Batch(device=device, max_slots=max_slots, max_items=max_slots, max_ells=3 * max_slots)
         self.reserved = 0            # footprint bounds of the resident contexts (admission)
         self.in_use = 0              # their actual device bytes
@@ -153,11 +161,18 @@ class Server:
                 if not joining and i < len(pending):
                     time.sleep(max(0.0, min(0.01, pending[i].arrival - now)))
                 continue
-            # one tick: the next slice of every admitted request in one batched launch
-            slices = []
-            for r in active:
+            # one tick: the next slice of the admitted requests in one batched launch
+            slices, given = [], {}
+            budget = self.tick_budget
+            for r in sorted(active, key=lambda q: q.arrival):
                 cnt = min(self.tick_packets, r.packets - r._next)
+                if self.policy == "fifo":
+                    if budget <= 0:
+                        break
+                    cnt = max(1, min(cnt, budget // 3))
+                    budget -= 3 * cnt
                 slices.append((r._ctx, [0, 1, 2], r.packets, r._next, cnt, r.seed))
+                given[r.rid] = cnt
             self.batch.run(A.PHASE_STELLAR, slices, precision=self.precision)
             # arrivals are admitted (contexts built on their own streams) while the tick runs
             admit(time.perf_counter() - t0, len(active))
@@ -166,7 +181,10 @@ class Server:
             now = time.perf_counter() - t0
             still = []
             for r in active:
-                r._next += min(self.tick_packets, r.packets - r._next)
+                if r.rid not in given:
+                    still.append(r)
+                    continue
+                r._next += given[r.rid]
                 r.ticks += 1
                 if r._next >= r.packets:
                     self._retire(r, time.perf_counter() - t0)

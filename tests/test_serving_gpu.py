@@ -37,3 +37,18 @@ def test_admission_by_memory_budget():
     # two 48^3 variants fit the budget, three do not; the bound holds for the real footprint
     assert srv.peak_resident == 2
     assert srv.peak_in_use <= 2 * est <= srv.budget
+
+
+def test_fifo_policy_serves_the_oldest_first():
+    """With the arrival-order policy and a tick budget of one slice, the admitted requests are run
+    one after another in arrival order (the longest wait is the shortest); their frames are still
+    the ones they give alone."""
+    reqs = serving.fitskirt_requests(n=5, rate=50.0, seed=9, packets=(2e4, 6e4), grid=(24, 32))
+    srv = serving.Server(max_slots=5, tick_packets=30000, npix=64, policy="fifo", tick_budget=3 * 30000)
+    done = srv.serve(reqs, realtime=False)
+    srv.close()
+    order = [r.rid for r in sorted(done, key=lambda r: r.done)]
+    assert order == [r.rid for r in sorted(reqs, key=lambda r: r.arrival)]
+    for r in done[:2]:
+        alone, _ = serving.run_alone(r, npix=64)
+        assert np.allclose(r.frame, alone, rtol=1e-10, atol=1e-12 * alone.max()), r.rid
