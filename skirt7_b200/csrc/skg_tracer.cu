@@ -65,6 +65,12 @@ namespace skg {
 // the event pass at 4 blocks of 256 per SM (64 registers, spilling part of the packet record):
 // its divergent, latency-bound code gains more from the warps than it loses to the spills
 // (octree disk, 10^7 packets: 34.6 ms against 45.2 ms at 2 blocks and 126 registers)
+// free records are relaunched by a launch pass of their own after the event pass, every lane of
+// its warps launching (octree disk, 10^7 packets: phase 185.8 against 194.4 ms; Cartesian 86.8
+// against 90.7 ms)
+#ifndef SKG_LAUNCH_KERNEL
+#define SKG_LAUNCH_KERNEL 1
+#endif
 #ifndef SKG_EVENT_MIN_BLOCKS
 #define SKG_EVENT_MIN_BLOCKS 4
 #endif
@@ -334,6 +340,88 @@ SKG_D int peel_jobs(const DevScene& S, int ell, bool scat, int cell, double kx, 
 
 constexpr int SED_PRIV = 1024;          // SED bins a block keeps privately (8 KB)
 
+// Free records take new packets (all lanes of the warp call this; `need` marks the lanes whose
+// record is free): one work-counter atomic per warp; a launch with zero luminosity takes the next
+// packet; a record finds none once the work counter is past the batch's packets.
+template<typename R>
+SKG_D void take_packets(const RunParams& P, const BatchHeader& H, int phase, bool peel_on, int lane, bool need,
+                        Packet& K, int& state, int& npeel, int& nmain, unsigned long long* s_cnt) {
+    const unsigned FULL = 0xffffffffu;
+    while (__any_sync(FULL, need)) {
+        const unsigned want = __ballot_sync(FULL, need);
+        const int leader = __ffs(want) - 1;
+        unsigned long long base = 0;
+        if (lane == leader) base = atomicAdd(P.work, (unsigned long long)__popc(want));
+        base = __shfl_sync(FULL, base, leader);
+        if (need) {
+            const uint64_t gp = base + __popc(want & ((1u << lane) - 1));
+            if (gp >= H.total) {
+                state = PK_DONE; need = false;
+            } else {
+                const int it = find_item(P.items, H.nitems, gp);
+                const WorkItem It = P.items[it];
+                const uint64_t q = gp - It.begin;
+                const int ei = (int)(q / It.count);
+                const uint64_t ip = It.first + (q - (uint64_t)ei * It.count);
+                const int ell = P.ells[It.ell0 + ei];
+                Philox rng;
+                rng.init(It.seed, ip, (uint32_t)ell | ((uint32_t)phase << 24));
+                atomicAdd(&s_cnt[C_PACKETS], 1ull);
+                const DevScene& S = *P.scenes[It.slot];
+                const Launched o = launch_packet(P.grids[It.slot], S, phase, ell, It.npp_total, rng);
+                if (o.ok) {
+                    K.x = (double)(R)o.x; K.y = (double)(R)o.y; K.z = (double)(R)o.z;
+                    K.kx = (double)(R)o.kx; K.ky = (double)(R)o.ky; K.kz = (double)(R)o.kz;
+                    K.L = o.L; K.Lth = o.Lth; K.s_int = 0;
+                    K.id = ip; K.item = it; K.ell = ell; K.nscatt = 0;
+                    K.pos_cell = -2; K.int_cell = -1; K.rngc = rng.c0;
+                    K.flags = pk_flags(o); K.peel_n = 0;
+                    npeel = peel_on ? peel_jobs<false>(S, ell, false, -1, 0, 0, 0, K.x, K.y, K.z, K.L, 0, 0, nullptr,
+                                                       nullptr)
+                                    : 0;
+                    nmain = S.ncomp > 0 ? 1 : 0;            // without dust the life cycle ends here
+                    state = nmain ? PK_WAIT : PK_TERM;
+                    need = false;
+                }
+            }
+        }
+    }
+}
+
+// Appends a packet's jobs (all lanes of the warp call this), one reservation per warp for each
+// kind: the path jobs (the longest) from index 0, a packet's peel-off jobs contiguous from index
+// npool on; counts the packets with work.
+SKG_D void append_jobs(const WaveParams& W, int p, Packet& K, int npeel, int nmain, bool scat_peel, double kx0,
+                       double ky0, double kz0, int lane) {
+    const unsigned FULL = 0xffffffffu;
+    int inm = nmain, inp = npeel;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int tm = __shfl_up_sync(FULL, inm, o), tp = __shfl_up_sync(FULL, inp, o);
+        if (lane >= o) { inm += tm; inp += tp; }
+    }
+    const int totm = __shfl_sync(FULL, inm, 31), totp = __shfl_sync(FULL, inp, 31);
+    unsigned bm = 0, bp = 0;
+    if (lane == 31) {
+        if (totm > 0) bm = atomicAdd(W.jcount, (unsigned)totm);
+        if (totp > 0) bp = atomicAdd(W.jcount + 1, (unsigned)totp);
+    }
+    bm = __shfl_sync(FULL, bm, 31);
+    bp = __shfl_sync(FULL, bp, 31);
+    const unsigned busy = __ballot_sync(FULL, npeel + nmain > 0);
+    if (lane == 0 && busy) {
+        atomicAdd(W.jcount + 3, (unsigned)__popc(busy));
+        atomicMax(W.last_busy, (unsigned)W.wave);
+    }
+    if (npeel > 0) {
+        const int j0 = W.npool + (int)(bp + inp - npeel);
+        const DevScene& S = *W.R.scenes[W.R.items[K.item].slot];
+        peel_jobs<true>(S, K.ell, scat_peel, K.int_cell, kx0, ky0, kz0, K.x, K.y, K.z, K.L, p, j0, W.jobs, W.jL);
+        K.peel_j0 = j0;
+    }
+    K.peel_n = npeel;
+    if (nmain) W.jobs[bm + inm - 1] = make_int2(p, JOB_MAIN);
+}
+
 template<typename R>
 __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 / SKG_EVENT_THREADS) event_kernel(const WaveParams W) {
     __shared__ unsigned long long s_cnt[C_N];
@@ -349,7 +437,9 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 
     const int phase = H.phase;
     const bool peel_on = phase != SKG_PHASE_DUST_SELFABS;
     const int lane = threadIdx.x & 31;
+#if SKG_LAUNCH_KERNEL
     const unsigned FULL = 0xffffffffu;
+#endif
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
 
     Packet K;
@@ -406,77 +496,27 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 
         state = PK_WAIT;
     }
 
-    // 3. free records take new packets: one work-counter atomic per warp; a launch with zero
-    //    luminosity takes the next packet
-    bool need = state == PK_EMPTY || state == PK_TERM;
-    while (__any_sync(FULL, need)) {
-        const unsigned want = __ballot_sync(FULL, need);
-        const int leader = __ffs(want) - 1;
-        unsigned long long base = 0;
-        if (lane == leader) base = atomicAdd(P.work, (unsigned long long)__popc(want));
-        base = __shfl_sync(FULL, base, leader);
-        if (need) {
-            const uint64_t gp = base + __popc(want & ((1u << lane) - 1));
-            if (gp >= H.total) {
-                state = PK_DONE; need = false;
-            } else {
-                const int it = find_item(P.items, H.nitems, gp);
-                const WorkItem It = P.items[it];
-                const uint64_t q = gp - It.begin;
-                const int ei = (int)(q / It.count);
-                const uint64_t ip = It.first + (q - (uint64_t)ei * It.count);
-                const int ell = P.ells[It.ell0 + ei];
-                Philox rng;
-                rng.init(It.seed, ip, (uint32_t)ell | ((uint32_t)phase << 24));
-                atomicAdd(&s_cnt[C_PACKETS], 1ull);
-                const DevScene& S = *P.scenes[It.slot];
-                const Launched o = launch_packet(P.grids[It.slot], S, phase, ell, It.npp_total, rng);
-                if (o.ok) {
-                    K.x = (double)(R)o.x; K.y = (double)(R)o.y; K.z = (double)(R)o.z;
-                    K.kx = (double)(R)o.kx; K.ky = (double)(R)o.ky; K.kz = (double)(R)o.kz;
-                    K.L = o.L; K.Lth = o.Lth; K.s_int = 0;
-                    K.id = ip; K.item = it; K.ell = ell; K.nscatt = 0;
-                    K.pos_cell = -2; K.int_cell = -1; K.rngc = rng.c0;
-                    K.flags = pk_flags(o); K.peel_n = 0;
-                    npeel = peel_on ? peel_jobs<false>(S, ell, false, -1, 0, 0, 0, K.x, K.y, K.z, K.L, 0, 0, nullptr,
-                                                       nullptr)
-                                    : 0;
-                    nmain = S.ncomp > 0 ? 1 : 0;            // without dust the life cycle ends here
-                    state = nmain ? PK_WAIT : PK_TERM;
-                    need = false;
-                }
-            }
+#if SKG_LAUNCH_KERNEL
+    // 3. free records go on the wave's free list: the launch pass gives them new packets, every
+    //    lane of its warps launching (here a warp's launches would run beside its scatterings)
+    {
+        const bool freed = p < W.npool && (state == PK_EMPTY || state == PK_TERM);
+        const unsigned fm = __ballot_sync(FULL, freed);
+        if (fm) {
+            const int leader = __ffs(fm) - 1;
+            unsigned base = 0;
+            if (lane == leader) base = atomicAdd(W.jcount + 5, (unsigned)__popc(fm));
+            base = __shfl_sync(FULL, base, leader);
+            if (freed) W.freelist[base + __popc(fm & ((1u << lane) - 1))] = p;
         }
     }
+#else
+    // 3. free records take new packets
+    take_packets<R>(P, H, phase, peel_on, lane, state == PK_EMPTY || state == PK_TERM, K, state, npeel, nmain, s_cnt);
+#endif
 
-    // 4. append the jobs, one reservation per warp for each kind: the path jobs (the longest)
-    //    from index 0, a packet's peel-off jobs contiguous from index npool on
-    int inm = nmain, inp = npeel;
-    for (int o = 1; o < 32; o <<= 1) {
-        const int tm = __shfl_up_sync(FULL, inm, o), tp = __shfl_up_sync(FULL, inp, o);
-        if (lane >= o) { inm += tm; inp += tp; }
-    }
-    const int totm = __shfl_sync(FULL, inm, 31), totp = __shfl_sync(FULL, inp, 31);
-    unsigned bm = 0, bp = 0;
-    if (lane == 31) {
-        if (totm > 0) bm = atomicAdd(W.jcount, (unsigned)totm);
-        if (totp > 0) bp = atomicAdd(W.jcount + 1, (unsigned)totp);
-    }
-    bm = __shfl_sync(FULL, bm, 31);
-    bp = __shfl_sync(FULL, bp, 31);
-    const unsigned busy = __ballot_sync(FULL, npeel + nmain > 0);
-    if (lane == 0 && busy) {
-        atomicAdd(W.jcount + 3, (unsigned)__popc(busy));
-        atomicMax(W.last_busy, (unsigned)W.wave);
-    }
-    if (npeel > 0) {
-        const int j0 = W.npool + (int)(bp + inp - npeel);
-        const DevScene& S = *P.scenes[P.items[K.item].slot];
-        peel_jobs<true>(S, K.ell, scat_peel, K.int_cell, kx0, ky0, kz0, K.x, K.y, K.z, K.L, p, j0, W.jobs, W.jL);
-        K.peel_j0 = j0;
-    }
-    K.peel_n = npeel;
-    if (nmain) W.jobs[bm + inm - 1] = make_int2(p, JOB_MAIN);
+    // 4. append the jobs
+    append_jobs(W, p, K, npeel, nmain, scat_peel, kx0, ky0, kz0, lane);
     if (p < W.npool && was_live) {
         K.flags = (K.flags & ~2) | (scat_peel ? 2 : 0);
         K.state = state;
@@ -494,6 +534,39 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 
             atomicAdd(S0.instr[i].sed + (t - S0.sed_base[i]), v);
         }
     }
+}
+
+// Launch pass: one thread per record the event pass freed, every lane of a warp launching
+// (StellarSystem::launch and the samplers, or the dust-emission launch), then the new packets'
+// jobs appended as the event pass does.
+template<typename R>
+__global__ void __launch_bounds__(SKG_EVENT_THREADS) launch_kernel(const WaveParams W) {
+    __shared__ unsigned long long s_cnt[C_N];
+    const RunParams& P = W.R;
+    const BatchHeader H = *P.hdr;
+    if (threadIdx.x < C_N) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int phase = H.phase;
+    const bool peel_on = phase != SKG_PHASE_DUST_SELFABS;
+    const int lane = threadIdx.x & 31;
+    const unsigned nfree = W.jcount[5];
+    for (unsigned b0 = blockIdx.x * blockDim.x; b0 < nfree; b0 += gridDim.x * blockDim.x) {
+        const unsigned i = b0 + threadIdx.x;
+        const bool mine = i < nfree;
+        const int p = mine ? W.freelist[i] : 0;
+        Packet K;
+        int state = PK_DONE, npeel = 0, nmain = 0;
+        if (mine) { K = W.pk[p]; state = K.state; }
+        take_packets<R>(P, H, phase, peel_on, lane, mine, K, state, npeel, nmain, s_cnt);
+        append_jobs(W, p, K, npeel, nmain, false, 0, 0, 0, lane);
+        if (mine) {
+            K.flags &= ~2;
+            K.state = state;
+            W.pk[p] = K;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < C_N && s_cnt[threadIdx.x]) atomicAdd(P.counters + threadIdx.x, s_cnt[threadIdx.x]);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -946,6 +1019,17 @@ template<typename R, template<typename> class Stepper>
 cudaError_t enqueue_wave(const WaveParams& W, int nslots, int trav_blocks, cudaEvent_t mid, cudaStream_t s) {
     const size_t smem = (size_t)nslots * sizeof(DevGrid);
     event_kernel<R><<<(W.npool + SKG_EVENT_THREADS - 1) / SKG_EVENT_THREADS, SKG_EVENT_THREADS, 0, s>>>(W);
+#if SKG_LAUNCH_KERNEL
+    {
+        static int sms = 0;
+        if (sms == 0) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        }
+        launch_kernel<R><<<sms * 16, SKG_EVENT_THREADS, 0, s>>>(W);
+    }
+#endif
     if (mid) cudaEventRecord(mid, s);
 #if SKG_SPLIT_TRAV
     // the path jobs, then the peel-off jobs in their lean kernel
@@ -1007,6 +1091,7 @@ WaveRunner::~WaveRunner() {
     for (cudaEvent_t e : ev_) cudaEventDestroy(e);
     for (cudaEvent_t e : tail_ev_) if (e) cudaEventDestroy(e);
     cudaFree(pk_);
+    cudaFree(free_);
     for (int b = 0; b < 2; b++) { cudaFree(jobs_[b]); cudaFree(jtau_[b]); cudaFree(jL_[b]); }
     cudaFree(ctr_);
     if (h_ctr_) cudaFreeHost(h_ctr_);
@@ -1021,8 +1106,9 @@ cudaError_t WaveRunner::reserve(size_t pool, int ngroups) {
         if ((e = cudaEventCreateWithFlags(&copied_, cudaEventDisableTiming)) != cudaSuccess) return e;
     }
     if (pool > cap_pool_) {
-        cudaFree(pk_); pk_ = nullptr; cap_pool_ = 0;
+        cudaFree(pk_); pk_ = nullptr; cudaFree(free_); free_ = nullptr; cap_pool_ = 0;
         if ((e = cudaMalloc(&pk_, pool * sizeof(Packet))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&free_, pool * sizeof(int))) != cudaSuccess) return e;
         cap_pool_ = pool;
     }
     const size_t jobs = pool * (size_t)(ngroups + 1);
@@ -1052,6 +1138,7 @@ cudaError_t WaveRunner::enqueue(int n) {
         W.jobs = jobs_[b]; W.jtau = jtau_[b]; W.jL = jL_[b]; W.jcount = ctr_ + 8 * b;
         W.pjobs = jobs_[b ^ 1]; W.pjtau = jtau_[b ^ 1]; W.pjL = jL_[b ^ 1];
         W.last_busy = ctr_ + 16;
+        W.freelist = free_;
         if ((e = cudaMemsetAsync(ctr_ + 8 * b, 0, 8 * sizeof(unsigned), stream_)) != cudaSuccess) return e;
         if (timed_) {
             while (ev_.size() < 3 * (size_t)(w + 1)) {
@@ -1097,6 +1184,7 @@ cudaError_t WaveRunner::enqueue_tail() {
     W.jobs = nullptr; W.jtau = nullptr; W.jL = nullptr; W.jcount = ctr_ + 8 * (b ^ 1);
     W.pjobs = jobs_[b]; W.pjtau = jtau_[b]; W.pjL = jL_[b];
     W.last_busy = ctr_ + 16;
+    W.freelist = nullptr;
     cudaError_t e;
     if (timed_) {
         for (int i = 0; i < 2; i++)

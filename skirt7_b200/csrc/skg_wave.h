@@ -52,6 +52,7 @@ private:
     cudaError_t enqueue_tail();
 
     Packet* pk_ = nullptr;
+    int* free_ = nullptr;             // records freed in a wave (the launch pass's work)
     size_t cap_pool_ = 0;
     int2* jobs_[2] = {nullptr, nullptr};
     double* jtau_[2] = {nullptr, nullptr};
