@@ -155,13 +155,14 @@ struct WaveParams {
     unsigned* jcount;                 // [0] path jobs, [1] peel-off jobs, [2] jobs taken by the
                                       // traversal pass (its path kernel when split), [3] packets
                                       // with jobs, [4] peel-off jobs taken by a split pass,
-                                      // [5] records on the free list
+                                      // [5] records on the free list, [6] on the interaction list
     // the previous wave's jobs (peel-off detection)
     const int2* pjobs;
     const double* pjtau;
     const double* pjL;
     unsigned* last_busy;              // highest wave index that had jobs
     int* freelist;                    // records the event pass freed (count: jcount[5])
+    int* intlist;                     // records it found at their interaction point (jcount[6])
 };
 
 // ---------------------------------------------------------------------------------------------

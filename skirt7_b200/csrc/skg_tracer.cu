@@ -9,12 +9,13 @@
 //   interaction point -> propagate -> peel-off (scattering) -> scatter -> path -> ...
 //
 // is cut at its traversals.  The packets in flight sit in a pool of 128-byte records.  Each wave
-// runs two kernels:
-//   event_kernel  one thread per record: detects the peel-offs walked in the previous wave, moves
-//                 a scattered packet to its interaction point, writes the scattering peel-offs,
-//                 scatters, or launches a new packet into a free record; then appends the packet's
-//                 next traversals to the wave's job list (one peel-off job per direction group and
-//                 one path job);
+// runs these kernels:
+//   event_kernel  one thread per record: detects the peel-offs walked in the previous wave and
+//                 lists the packets at their interaction point and the free records;
+//   launch_kernel one thread per listed record: moves a packet to its interaction point, writes
+//                 its scattering peel-offs and scatters it, or launches a new packet into a free
+//                 record; then appends the packet's next traversals to the wave's job list (one
+//                 peel-off job per direction group and one path job);
 //   trav_kernel   persistent, launched twice (the path jobs, then the peel-off jobs in a lean
 //                 instantiation); each lane takes jobs one after another and walks them:
 //                 peel-off  accumulates the optical depth towards an observer
@@ -65,9 +66,9 @@ namespace skg {
 // the event pass at 4 blocks of 256 per SM (64 registers, spilling part of the packet record):
 // its divergent, latency-bound code gains more from the warps than it loses to the spills
 // (octree disk, 10^7 packets: 34.6 ms against 45.2 ms at 2 blocks and 126 registers)
-// free records are relaunched by a launch pass of their own after the event pass, every lane of
-// its warps launching (octree disk, 10^7 packets: phase 185.8 against 194.4 ms; Cartesian 86.8
-// against 90.7 ms)
+// packets at their interaction point and free records are scattered and relaunched by a pass of
+// their own after the event pass, every lane of its warps doing the same work (octree disk, 10^7
+// packets: phase 177.7 against 194.4 ms in one event pass; Cartesian 87.0 against 90.7 ms)
 #ifndef SKG_LAUNCH_KERNEL
 #define SKG_LAUNCH_KERNEL 1
 #endif
@@ -340,6 +341,36 @@ SKG_D int peel_jobs(const DevScene& S, int ell, bool scat, int cell, double kx, 
 
 constexpr int SED_PRIV = 1024;          // SED bins a block keeps privately (8 KB)
 
+// A packet at its interaction point: propagate, count its scattering peel-offs, scatter
+// (simulatepropagation :513-531, peeloffscattering :313-357, simulatescattering :535-543).
+template<typename R>
+SKG_D void scatter_packet(const RunParams& P, int phase, bool peel_on, Packet& K, int& state, int& npeel, int& nmain,
+                          bool& scat_peel, double& kx0, double& ky0, double& kz0, unsigned long long* s_cnt) {
+    const WorkItem& It = P.items[K.item];
+    const DevScene& S = *P.scenes[It.slot];
+    const R si = (R)K.s_int;                        // PhotonPackage::propagate
+    K.x = (double)((R)K.x + si * (R)K.kx);
+    K.y = (double)((R)K.y + si * (R)K.ky);
+    K.z = (double)((R)K.z + si * (R)K.kz);
+    // the interaction point lies in the cell of its segment (verified by the stepper)
+    if (K.s_int > 0) K.pos_cell = (K.int_cell >= 0) ? K.int_cell : -2;
+    kx0 = K.kx; ky0 = K.ky; kz0 = K.kz;
+    if (peel_on) {
+        scat_peel = true;
+        npeel = peel_jobs<false>(S, K.ell, true, K.int_cell, kx0, ky0, kz0, K.x, K.y, K.z, K.L, 0, 0, nullptr, nullptr);
+    }
+    Philox rng;
+    rng.init(It.seed, K.id, (uint32_t)K.ell | ((uint32_t)phase << 24));
+    rng.c0 = K.rngc;
+    const V3<double> kn = scatter_direction(S, K.ell, K.int_cell, mk3(K.kx, K.ky, K.kz), rng);
+    K.rngc = rng.c0;
+    K.kx = (double)(R)kn.x; K.ky = (double)(R)kn.y; K.kz = (double)(R)kn.z;
+    K.nscatt++;
+    atomicAdd(&s_cnt[C_SCATT], 1ull);
+    nmain = 1;
+    state = PK_WAIT;
+}
+
 // Free records take new packets (all lanes of the warp call this; `need` marks the lanes whose
 // record is free): one work-counter atomic per warp; a launch with zero luminosity takes the next
 // packet; a record finds none once the work counter is past the batch's packets.
@@ -434,8 +465,10 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 
     if (threadIdx.x < C_N) s_cnt[threadIdx.x] = 0;
     if (psed) for (int t = threadIdx.x; t < sed_bins; t += blockDim.x) s_sed[t] = 0.0;
     __syncthreads();
+#if !SKG_LAUNCH_KERNEL
     const int phase = H.phase;
     const bool peel_on = phase != SKG_PHASE_DUST_SELFABS;
+#endif
     const int lane = threadIdx.x & 31;
 #if SKG_LAUNCH_KERNEL
     const unsigned FULL = 0xffffffffu;
@@ -469,32 +502,23 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 
     int npeel = 0, nmain = 0;
     bool scat_peel = false;
     double kx0 = 0, ky0 = 0, kz0 = 0;              // direction before the scattering
-    if (state == PK_INTERACT) {
-        const WorkItem& It = P.items[K.item];
-        const DevScene& S = *P.scenes[It.slot];
-        const R si = (R)K.s_int;                    // PhotonPackage::propagate
-        K.x = (double)((R)K.x + si * (R)K.kx);
-        K.y = (double)((R)K.y + si * (R)K.ky);
-        K.z = (double)((R)K.z + si * (R)K.kz);
-        // the interaction point lies in the cell of its segment (verified by the stepper)
-        if (K.s_int > 0) K.pos_cell = (K.int_cell >= 0) ? K.int_cell : -2;
-        kx0 = K.kx; ky0 = K.ky; kz0 = K.kz;
-        if (peel_on) {
-            scat_peel = true;
-            npeel = peel_jobs<false>(S, K.ell, true, K.int_cell, kx0, ky0, kz0, K.x, K.y, K.z, K.L, 0, 0, nullptr,
-                                     nullptr);
+#if SKG_LAUNCH_KERNEL
+    // (in the launch pass, with every lane of its warps scattering)
+    {
+        const bool inter = p < W.npool && state == PK_INTERACT;
+        const unsigned im = __ballot_sync(FULL, inter);
+        if (im) {
+            const int leader = __ffs(im) - 1;
+            unsigned base = 0;
+            if (lane == leader) base = atomicAdd(W.jcount + 6, (unsigned)__popc(im));
+            base = __shfl_sync(FULL, base, leader);
+            if (inter) W.intlist[base + __popc(im & ((1u << lane) - 1))] = p;
         }
-        Philox rng;
-        rng.init(It.seed, K.id, (uint32_t)K.ell | ((uint32_t)phase << 24));
-        rng.c0 = K.rngc;
-        const V3<double> kn = scatter_direction(S, K.ell, K.int_cell, mk3(K.kx, K.ky, K.kz), rng);
-        K.rngc = rng.c0;
-        K.kx = (double)(R)kn.x; K.ky = (double)(R)kn.y; K.kz = (double)(R)kn.z;
-        K.nscatt++;
-        atomicAdd(&s_cnt[C_SCATT], 1ull);
-        nmain = 1;
-        state = PK_WAIT;
     }
+#else
+    if (state == PK_INTERACT)
+        scatter_packet<R>(P, phase, peel_on, K, state, npeel, nmain, scat_peel, kx0, ky0, kz0, s_cnt);
+#endif
 
 #if SKG_LAUNCH_KERNEL
     // 3. free records go on the wave's free list: the launch pass gives them new packets, every
@@ -515,6 +539,11 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 
     take_packets<R>(P, H, phase, peel_on, lane, state == PK_EMPTY || state == PK_TERM, K, state, npeel, nmain, s_cnt);
 #endif
 
+#if SKG_LAUNCH_KERNEL
+    // every live record is now on one of the two lists, and the scatter-and-launch pass rewrites
+    // it (jobs, state, the cleared peel-off count): this pass only read it
+    (void)npeel; (void)nmain; (void)scat_peel; (void)kx0; (void)ky0; (void)kz0; (void)was_live;
+#else
     // 4. append the jobs
     append_jobs(W, p, K, npeel, nmain, scat_peel, kx0, ky0, kz0, lane);
     if (p < W.npool && was_live) {
@@ -522,6 +551,7 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 
         K.state = state;
         W.pk[p] = K;
     }
+#endif
     __syncthreads();
     if (threadIdx.x < C_N && s_cnt[threadIdx.x]) atomicAdd(P.counters + threadIdx.x, s_cnt[threadIdx.x]);
     if (psed) {
@@ -536,9 +566,10 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 
     }
 }
 
-// Launch pass: one thread per record the event pass freed, every lane of a warp launching
-// (StellarSystem::launch and the samplers, or the dust-emission launch), then the new packets'
-// jobs appended as the event pass does.
+// Scatter-and-launch pass: one thread per record the event pass found at its interaction point
+// (propagation, scattering peel-offs, scattering), then one per record it freed (StellarSystem::launch
+// and the samplers, or the dust-emission launch), every lane of a warp doing the same work; the
+// packets' jobs are appended as the event pass does.
 template<typename R>
 __global__ void __launch_bounds__(SKG_EVENT_THREADS) launch_kernel(const WaveParams W) {
     __shared__ unsigned long long s_cnt[C_N];
@@ -549,6 +580,27 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS) launch_kernel(const WavePar
     const int phase = H.phase;
     const bool peel_on = phase != SKG_PHASE_DUST_SELFABS;
     const int lane = threadIdx.x & 31;
+    const unsigned nint = W.jcount[6];
+    for (unsigned b0 = blockIdx.x * blockDim.x; b0 < nint; b0 += gridDim.x * blockDim.x) {
+        const unsigned i = b0 + threadIdx.x;
+        const bool mine = i < nint;
+        const int p = mine ? W.intlist[i] : 0;
+        Packet K;
+        int state = PK_DONE, npeel = 0, nmain = 0;
+        bool scat_peel = false;
+        double kx0 = 0, ky0 = 0, kz0 = 0;
+        if (mine) {
+            K = W.pk[p];
+            state = K.state;
+            scatter_packet<R>(P, phase, peel_on, K, state, npeel, nmain, scat_peel, kx0, ky0, kz0, s_cnt);
+        }
+        append_jobs(W, p, K, npeel, nmain, scat_peel, kx0, ky0, kz0, lane);
+        if (mine) {
+            K.flags = (K.flags & ~2) | (scat_peel ? 2 : 0);   // the pending peel-offs follow a scattering
+            K.state = state;
+            W.pk[p] = K;
+        }
+    }
     const unsigned nfree = W.jcount[5];
     for (unsigned b0 = blockIdx.x * blockDim.x; b0 < nfree; b0 += gridDim.x * blockDim.x) {
         const unsigned i = b0 + threadIdx.x;
@@ -1108,7 +1160,7 @@ cudaError_t WaveRunner::reserve(size_t pool, int ngroups) {
     if (pool > cap_pool_) {
         cudaFree(pk_); pk_ = nullptr; cudaFree(free_); free_ = nullptr; cap_pool_ = 0;
         if ((e = cudaMalloc(&pk_, pool * sizeof(Packet))) != cudaSuccess) return e;
-        if ((e = cudaMalloc(&free_, pool * sizeof(int))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&free_, 2 * pool * sizeof(int))) != cudaSuccess) return e;
         cap_pool_ = pool;
     }
     const size_t jobs = pool * (size_t)(ngroups + 1);
@@ -1138,7 +1190,7 @@ cudaError_t WaveRunner::enqueue(int n) {
         W.jobs = jobs_[b]; W.jtau = jtau_[b]; W.jL = jL_[b]; W.jcount = ctr_ + 8 * b;
         W.pjobs = jobs_[b ^ 1]; W.pjtau = jtau_[b ^ 1]; W.pjL = jL_[b ^ 1];
         W.last_busy = ctr_ + 16;
-        W.freelist = free_;
+        W.freelist = free_; W.intlist = free_ + npool_;
         if ((e = cudaMemsetAsync(ctr_ + 8 * b, 0, 8 * sizeof(unsigned), stream_)) != cudaSuccess) return e;
         if (timed_) {
             while (ev_.size() < 3 * (size_t)(w + 1)) {
@@ -1184,7 +1236,7 @@ cudaError_t WaveRunner::enqueue_tail() {
     W.jobs = nullptr; W.jtau = nullptr; W.jL = nullptr; W.jcount = ctr_ + 8 * (b ^ 1);
     W.pjobs = jobs_[b]; W.pjtau = jtau_[b]; W.pjL = jL_[b];
     W.last_busy = ctr_ + 16;
-    W.freelist = nullptr;
+    W.freelist = nullptr; W.intlist = nullptr;
     cudaError_t e;
     if (timed_) {
         for (int i = 0; i < 2; i++)

@@ -52,7 +52,8 @@ private:
     cudaError_t enqueue_tail();
 
     Packet* pk_ = nullptr;
-    int* free_ = nullptr;             // records freed in a wave (the launch pass's work)
+    int* free_ = nullptr;             // [pool] records freed in a wave, [pool] records at their
+                                      // interaction point (the scatter-and-launch pass's work)
     size_t cap_pool_ = 0;
     int2* jobs_[2] = {nullptr, nullptr};
     double* jtau_[2] = {nullptr, nullptr};
