@@ -444,8 +444,9 @@ def main():
                          "phase_ms": kms, "event_pass_ms": ev_ms, "traversal_pass_ms": trav_ms},
             "e2e": {"value": e2e, "unit": "packets/s", "h2d_bytes_per_step": len(phases) * (4 * nl + 64),
                     "d2h_bytes_per_step": cubes_bytes},
-            # per wave: the event pass and the two traversal kernels (path jobs, peel-off jobs)
-            "gpu_launches": 3 * waves * len(phases) * args.steps,
+            # per wave: the event pass, the scatter-and-launch pass and the two traversal kernels
+            # (path jobs, peel-off jobs)
+            "gpu_launches": 4 * waves * len(phases) * args.steps,
             "clocks": clk,
             "counters_stellar_phase": c,
         }
@@ -486,6 +487,7 @@ def serving_leg(args, device):
     return {"requests": len(reqs), "arrival_rate_per_s": 20.0, "p50_s": st["p50_s"], "p99_s": st["p99_s"],
             "alone_p50_s": a50, "alone_p99_s": a99, "p99_over_alone_p99": st["p99_s"] / a99,
             "packets_per_s": packets / wall, "makespan_s": wall, "ticks": srv.ticks,
+            "tick_device_s": srv.tick_gpu_s, "admit_host_s": srv.admit_s,
             "peak_resident": srv.peak_resident}
 
 

@@ -737,7 +737,7 @@ int skg_run_phase(skg_ctx* ctx, int phase, const int32_t* ells, int nell, uint64
         const uint64_t total = (uint64_t)nell * count;
         const size_t pool_max = (opts && opts->pool > 0) ? (size_t)opts->pool : ((size_t)1 << 21);
         const size_t npool = (size_t)std::min<uint64_t>(total, pool_max);
-        CK(ctx->waves.reserve(npool, ctx->hs.ngroups));
+        CK(ctx->waves.reserve(npool, ctx->hs.ngroups, ctx->grid.type));
         // one slot, one work item (pageable host sources: the copies are staged before return)
         BatchHeader H = {phase, 1, 1, 0, total};
         WorkItem W;
@@ -1202,7 +1202,7 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
         int ngroups = 0;
         for (skg_ctx* c : slots) ngroups = std::max(ngroups, c->hs.ngroups);
         if (total == 0) return SKG_OK;
-        CK(b->waves.reserve(npool, ngroups));
+        CK(b->waves.reserve(npool, ngroups, gtype));
         RunParams P = b->T.params((opts && opts->max_scatt > 0) ? opts->max_scatt : 100000);
         Staging& T = b->T;
         auto enqueue = [&](cudaStream_t q) {

@@ -163,6 +163,7 @@ struct WaveParams {
     unsigned* last_busy;              // highest wave index that had jobs
     int* freelist;                    // records the event pass freed (count: jcount[5])
     int* intlist;                     // records it found at their interaction point (jcount[6])
+    float4* ckpt;                     // per packet record: checkpoints of its path walk
 };
 
 // ---------------------------------------------------------------------------------------------

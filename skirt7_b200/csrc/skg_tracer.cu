@@ -98,6 +98,27 @@ namespace skg {
 #ifndef SKG_REFILL_PEEL
 #define SKG_REFILL_PEEL SKG_REFILL_LANES
 #endif
+// checkpoints of a path's walk (FP32 steppers that can resume): every SKG_CKPT_STRIDE cell steps,
+// up to SKG_CKPT_N per packet record, the walk stores its state with the optical depth and path
+// length so far; the re-walk to the interaction point then starts at the last checkpoint below the
+// interaction optical depth (at most one stride of cell steps) instead of at the path's start
+#ifndef SKG_CKPT
+#define SKG_CKPT 1
+#endif
+// cell steps a lane takes per pass of the traversal loop (the warp's refill and end-of-path votes
+// run once per pass): peel-off-job kernel, path-job kernel
+#ifndef SKG_INNER_STEPS
+#define SKG_INNER_STEPS 1
+#endif
+#ifndef SKG_INNER_PATH
+#define SKG_INNER_PATH 1
+#endif
+#ifndef SKG_CKPT_N
+#define SKG_CKPT_N 32
+#endif
+#ifndef SKG_CKPT_STRIDE
+#define SKG_CKPT_STRIDE 16
+#endif
 
 enum Cnt : int { C_PACKETS = 0, C_STEPS, C_TRAV, C_SCATT, C_PEEL, C_ABS, C_PIX, C_NBR, C_FB, C_ERR, C_N };
 
@@ -119,7 +140,15 @@ template<typename R> SKG_D double kappa_rho(const DevScene& S, int m, int ell) {
 // FullInstrument.cpp:109-177).  SED bins go to the block's private copy `psed` when it is given
 // (every packet of a wavelength adds to the same SED bin: global atomics would serialise on it).
 // Returns the number of tally updates.
-__device__ __noinline__ int detect_group(const DevScene& S, int grp, int ell, double Lpeel, double tau,
+#ifndef SKG_DETECT_INLINE
+#define SKG_DETECT_INLINE 0
+#endif
+#if SKG_DETECT_INLINE
+__device__ __forceinline__
+#else
+__device__ __noinline__
+#endif
+int detect_group(const DevScene& S, int grp, int ell, double Lpeel, double tau,
                                          int nscatt_peel, bool stellar, int comp, double x, double y, double z,
                                          double* psed) {
     double Lextf = Lpeel * exp(-tau);
@@ -692,6 +721,41 @@ SKG_D int after_path(const WaveParams& W, const DevScene& S, int p, int phase, i
     return 1;
 }
 
+// A checkpoint of packet p's path walk (slot i): the stepper's state, then the optical depth and
+// the path length walked (from the packet's position) and the step count.
+template<class St>
+SKG_D void save_ckpt(const WaveParams& W, int p, int i, const St& st, double tau) {
+    const Packet& K = W.pk[p];
+    const float s = st.walked_from((float)K.x, (float)K.y, (float)K.z);
+    float4* c = W.ckpt + ((size_t)p * SKG_CKPT_N + i) * 2;
+    c[0] = st.ckpt();
+    c[1] = make_float4(__int_as_float(__double2loint(tau)), __int_as_float(__double2hiint(tau)), s,
+                       __int_as_float(st.steps));
+}
+
+// Resumes the re-walk of packet p's path toward tau_int at its last checkpoint (of nck) whose
+// optical depth is at most tau_int: the steps before it would not have reached tau_int.  Returns
+// false when there is none (the re-walk starts at the path's start).
+template<class St>
+SKG_D bool resume_ckpt(const WaveParams& W, const DevGrid& g, int p, int nck, double tau_int, St& st, double& tau,
+                       double& s) {
+    const float4* c = W.ckpt + (size_t)p * SKG_CKPT_N * 2;
+    int lo = -1, hi = nck - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const float4 b = c[2 * mid + 1];
+        if (__hiloint2double(__float_as_int(b.y), __float_as_int(b.x)) <= tau_int) lo = mid; else hi = mid - 1;
+    }
+    if (lo < 0) return false;
+    const float4 b = c[2 * lo + 1];
+    const Packet& K = W.pk[p];
+    st.resume(g, (float)K.x, (float)K.y, (float)K.z, (float)K.kx, (float)K.ky, (float)K.kz, K.pos_cell, c[2 * lo],
+              __float_as_int(b.w));
+    tau = __hiloint2double(__float_as_int(b.y), __float_as_int(b.x));
+    s = (double)b.z;
+    return true;
+}
+
 // MODE: 0 every job of the wave; 1 the path jobs only; 2 the peel-off jobs only (a lean
 // instantiation: optical depth alone, no path state)
 // Resident blocks per SM of each instantiation.  The Voronoi path-job kernel runs at 3 blocks (80
@@ -739,6 +803,8 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
     float kext1 = -1.f;               // kappa_ext at the job's wavelength (one dust component), else -1
     unsigned c_steps = 0;
     Stepper<R> st;
+    constexpr bool CKPT = SKG_CKPT && MODE != 2 && Resumable<Stepper<R>>::value;
+    int nck = 0;                      // checkpoints of the path walk
 
     while (true) {
         // lanes without a job take the next ones: one atomic per warp
@@ -755,11 +821,16 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
                 double L = W.pk[p].L, tau_int = 0;      // the packet's luminosity at the path start
                 const int rc = after_path(W, S, p, phase, ell, tau, v2, L, tau_int);
                 if (rc == 1) {
-                    const Packet& K = W.pk[p];
-                    st.init(g, (R)K.x, (R)K.y, (R)K.z, (R)K.kx, (R)K.ky, (R)K.kz, K.pos_cell);
-                    tau = 0; v1 = 0; v2 = tau_int; kind = 2;
-                    R d0;
-                    while (st.pd.pop(d0)) v1 += (double)d0;
+                    kind = 2; v2 = tau_int;
+                    bool resumed = false;
+                    if constexpr (CKPT) resumed = W.ckpt && resume_ckpt(W, g, p, nck, tau_int, st, tau, v1);
+                    if (!resumed) {
+                        const Packet& K = W.pk[p];
+                        st.init(g, (R)K.x, (R)K.y, (R)K.z, (R)K.kx, (R)K.ky, (R)K.kz, K.pos_cell);
+                        tau = 0; v1 = 0;
+                        R d0;
+                        while (st.pd.pop(d0)) v1 += (double)d0;
+                    }
                 } else {
                     if (rc < 0) atomicAdd(&s_cnt[C_ERR], 1ull);
                     j = -1;
@@ -788,7 +859,7 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
                 const int hint = K.pos_cell;
                 kext1 = (S.ncomp == 1) ? (float)S.kext[ell] : -1.f;
                 R kx, ky, kz;
-                if (MODE != 2 && jb.y == JOB_MAIN) { kx = (R)K.kx; ky = (R)K.ky; kz = (R)K.kz; kind = 1; v1 = K.L; v2 = 0; }
+                if (MODE != 2 && jb.y == JOB_MAIN) { kx = (R)K.kx; ky = (R)K.ky; kz = (R)K.kz; kind = 1; v1 = K.L; v2 = 0; nck = 0; }
                 else { kx = (R)S.gkx[jb.y]; ky = (R)S.gky[jb.y]; kz = (R)S.gkz[jb.y]; kind = 0; }
                 st.init(sg[slot], (R)K.x, (R)K.y, (R)K.z, kx, ky, kz, hint);
                 if (kind == 1 && hint == -2) W.pk[p].pos_cell = st.cell0;
@@ -800,51 +871,62 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
 
         if (j < 0 || kind == 3) continue;   // waiting for enough lanes to refill / end paths together
 
-        // one cell step
+        // cell steps: up to SKG_INNER_STEPS of them before the warp looks at refills again
         const DevGrid& g = sg[slot];
         const DevScene& S = *s_scene[slot];
-        int m; R ds;
-        if (st.walk(g, m, ds)) {
-            c_steps++;
-            // one dust component: the FP32 tree walk carries the cell density in its leaf record
-            const double kr = (kext1 >= 0.f && st.rho >= 0.f) ? (double)(kext1 * st.rho) : kappa_rho<R>(S, m, ell);
-            const double dtau = kr * (double)ds;
-            if (kind == 0) {
-                tau += dtau;
-            } else if (kind == 1) {
-                if (absorb_step<R>(S, phase, m, ell, dtau, v1, v2)) atomicAdd(&s_cnt[C_ABS], 1ull);
-                tau += dtau;
-            } else {
-                const double tn = tau + dtau, sn = v1 + (double)ds;
-                if (tn > v2) {
-                    Packet& K = W.pk[p];
-                    K.s_int = v1 + ((v2 - tau) / (tn - tau)) * (sn - v1);
-                    K.int_cell = m;
-                    K.state = PK_INTERACT;
-                    atomicAdd(&s_cnt[C_TRAV], 1ull);
-                    atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.nscanned());
-                    atomicAdd(&s_cnt[C_FB], (unsigned long long)st.fallbacks);
-                    j = -1;
+#pragma unroll 1
+        for (int is = 0; is < (MODE == 2 ? SKG_INNER_STEPS : SKG_INNER_PATH); is++) {
+            int m; R ds;
+            if (st.walk(g, m, ds)) {
+                c_steps++;
+                // one dust component: the FP32 tree walk carries the cell density in its leaf record
+                const double kr = (kext1 >= 0.f && st.rho >= 0.f) ? (double)(kext1 * st.rho) : kappa_rho<R>(S, m, ell);
+                const double dtau = kr * (double)ds;
+                if (kind == 0) {
+                    tau += dtau;
+                } else if (kind == 1) {
+                    if (absorb_step<R>(S, phase, m, ell, dtau, v1, v2)) atomicAdd(&s_cnt[C_ABS], 1ull);
+                    tau += dtau;
+                    if constexpr (CKPT) {
+                        if (W.ckpt && nck < SKG_CKPT_N && st.steps >= (nck + 1) * SKG_CKPT_STRIDE && !st.done) {
+                            save_ckpt(W, p, nck, st, tau);
+                            nck++;
+                        }
+                    }
                 } else {
-                    tau = tn; v1 = sn;
+                    const double tn = tau + dtau, sn = v1 + (double)ds;
+                    if (tn > v2) {
+                        Packet& K = W.pk[p];
+                        K.s_int = v1 + ((v2 - tau) / (tn - tau)) * (sn - v1);
+                        K.int_cell = m;
+                        K.state = PK_INTERACT;
+                        atomicAdd(&s_cnt[C_TRAV], 1ull);
+                        atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.nscanned());
+                        atomicAdd(&s_cnt[C_FB], (unsigned long long)st.fallbacks);
+                        j = -1;
+                        break;
+                    } else {
+                        tau = tn; v1 = sn;
+                    }
                 }
-            }
-        } else {
-            // the traversal reached the edge of the grid
-            atomicAdd(&s_cnt[C_TRAV], 1ull);
-            atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.nscanned());
-            atomicAdd(&s_cnt[C_FB], (unsigned long long)st.fallbacks);
-            if (st.steps > g.max_steps) { atomicOr(P.err, ERR_STEP_BUDGET); atomicAdd(&s_cnt[C_ERR], 1ull); }
-            if (kind == 0) {
-                W.jtau[j] = tau;
-                j = -1;
-            } else if (kind == 1) {
-                kind = 3;                       // the end of the path runs with other lanes' (above)
             } else {
-                // DustGridPath::pathlength: an optical depth beyond the last segment gives the full length
-                Packet& K = W.pk[p];
-                K.s_int = v1; K.int_cell = -1; K.state = PK_INTERACT;
-                j = -1;
+                // the traversal reached the edge of the grid
+                atomicAdd(&s_cnt[C_TRAV], 1ull);
+                atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.nscanned());
+                atomicAdd(&s_cnt[C_FB], (unsigned long long)st.fallbacks);
+                if (st.steps > g.max_steps) { atomicOr(P.err, ERR_STEP_BUDGET); atomicAdd(&s_cnt[C_ERR], 1ull); }
+                if (kind == 0) {
+                    W.jtau[j] = tau;
+                    j = -1;
+                } else if (kind == 1) {
+                    kind = 3;                       // the end of the path runs with other lanes' (above)
+                } else {
+                    // DustGridPath::pathlength: an optical depth beyond the last segment gives the full length
+                    Packet& K = W.pk[p];
+                    K.s_int = v1; K.int_cell = -1; K.state = PK_INTERACT;
+                    j = -1;
+                }
+                break;
             }
         }
     }
@@ -925,6 +1007,8 @@ SKG_D void tail_path(const WaveParams& W, const DevGrid& g, const DevScene& S, i
     st.init(g, (R)K.x, (R)K.y, (R)K.z, (R)K.kx, (R)K.ky, (R)K.kz, hint);
     if (hint == -2) K.pos_cell = st.cell0;
     double tau = 0, v1 = K.L, v2 = 0;
+    constexpr bool CKPT = SKG_CKPT && Resumable<Stepper<R>>::value;
+    int nck = 0;                                  // checkpoints, as the traversal pass takes them
     int m; R ds;
     while (st.walk(g, m, ds)) {
         cnt[C_STEPS]++;
@@ -932,6 +1016,12 @@ SKG_D void tail_path(const WaveParams& W, const DevGrid& g, const DevScene& S, i
         const double dtau = kr * (double)ds;
         cnt[C_ABS] += absorb_step<R>(S, phase, m, ell, dtau, v1, v2);
         tau += dtau;
+        if constexpr (CKPT) {
+            if (W.ckpt && nck < SKG_CKPT_N && st.steps >= (nck + 1) * SKG_CKPT_STRIDE && !st.done) {
+                save_ckpt(W, p, nck, st, tau);
+                nck++;
+            }
+        }
     }
     cnt[C_TRAV]++; cnt[C_NBR] += st.nscanned(); cnt[C_FB] += st.fallbacks;
     if (st.steps > g.max_steps) { atomicOr(W.R.err, ERR_STEP_BUDGET); cnt[C_ERR]++; }
@@ -940,11 +1030,15 @@ SKG_D void tail_path(const WaveParams& W, const DevGrid& g, const DevScene& S, i
     if (rc < 0) cnt[C_ERR]++;
     if (rc != 1) return;
     // DustGridPath::pathlength on the re-walked path
-    st.init(g, (R)K.x, (R)K.y, (R)K.z, (R)K.kx, (R)K.ky, (R)K.kz, K.pos_cell);
     double s = 0;
-    R d0;
-    while (st.pd.pop(d0)) s += (double)d0;
-    tau = 0;
+    bool resumed = false;
+    if constexpr (CKPT) resumed = W.ckpt && resume_ckpt(W, g, p, nck, tau_int, st, tau, s);
+    if (!resumed) {
+        st.init(g, (R)K.x, (R)K.y, (R)K.z, (R)K.kx, (R)K.ky, (R)K.kz, K.pos_cell);
+        R d0;
+        while (st.pd.pop(d0)) s += (double)d0;
+        tau = 0;
+    }
     while (st.walk(g, m, ds)) {
         cnt[C_STEPS]++;
         const double kr = (kext1 >= 0.f && st.rho >= 0.f) ? (double)(kext1 * st.rho) : kappa_rho<R>(S, m, ell);
@@ -1144,13 +1238,21 @@ WaveRunner::~WaveRunner() {
     for (cudaEvent_t e : tail_ev_) if (e) cudaEventDestroy(e);
     cudaFree(pk_);
     cudaFree(free_);
+    cudaFree(ckpt_);
     for (int b = 0; b < 2; b++) { cudaFree(jobs_[b]); cudaFree(jtau_[b]); cudaFree(jL_[b]); }
     cudaFree(ctr_);
     if (h_ctr_) cudaFreeHost(h_ctr_);
     if (copied_) cudaEventDestroy(copied_);
 }
 
-cudaError_t WaveRunner::reserve(size_t pool, int ngroups) {
+// grids whose FP32 walk resumes from checkpoints (the steppers' Resumable trait)
+static bool ckpt_grid(int grid_type) {
+    if (grid_type == SKG_GRID_VORONOI) return Resumable<VoronoiStepper<float>>::value;
+    if (grid_type == SKG_GRID_CARTESIAN) return Resumable<CartStepper<float>>::value;
+    return Resumable<TreeLatticeStepper<float>>::value;
+}
+
+cudaError_t WaveRunner::reserve(size_t pool, int ngroups, int grid_type) {
     cudaError_t e;
     if (!ctr_) {
         if ((e = cudaMalloc(&ctr_, NCTR * sizeof(unsigned))) != cudaSuccess) return e;
@@ -1162,6 +1264,11 @@ cudaError_t WaveRunner::reserve(size_t pool, int ngroups) {
         if ((e = cudaMalloc(&pk_, pool * sizeof(Packet))) != cudaSuccess) return e;
         if ((e = cudaMalloc(&free_, 2 * pool * sizeof(int))) != cudaSuccess) return e;
         cap_pool_ = pool;
+    }
+    if (SKG_CKPT && ckpt_grid(grid_type) && pool > cap_ckpt_) {
+        cudaFree(ckpt_); ckpt_ = nullptr; cap_ckpt_ = 0;
+        if ((e = cudaMalloc(&ckpt_, pool * SKG_CKPT_N * 2 * sizeof(float4))) != cudaSuccess) return e;
+        cap_ckpt_ = pool;
     }
     const size_t jobs = pool * (size_t)(ngroups + 1);
     if (jobs > cap_jobs_) {
@@ -1190,7 +1297,7 @@ cudaError_t WaveRunner::enqueue(int n) {
         W.jobs = jobs_[b]; W.jtau = jtau_[b]; W.jL = jL_[b]; W.jcount = ctr_ + 8 * b;
         W.pjobs = jobs_[b ^ 1]; W.pjtau = jtau_[b ^ 1]; W.pjL = jL_[b ^ 1];
         W.last_busy = ctr_ + 16;
-        W.freelist = free_; W.intlist = free_ + npool_;
+        W.freelist = free_; W.intlist = free_ + npool_; W.ckpt = ckpt_on_ ? ckpt_ : nullptr;
         if ((e = cudaMemsetAsync(ctr_ + 8 * b, 0, 8 * sizeof(unsigned), stream_)) != cudaSuccess) return e;
         if (timed_) {
             while (ev_.size() < 3 * (size_t)(w + 1)) {
@@ -1219,6 +1326,8 @@ cudaError_t WaveRunner::begin(const RunParams& P, int grid_type, int tree_walk, 
     trav_blocks_ = trav_blocks; stream_ = s; npool_ = (int)npool; waves_ = 0; tail_ran_ = false;
     const char* td = std::getenv("SKG_TAIL_DIV");
     tail_div_ = td ? std::atoi(td) : tail_div;
+    const char* ck = std::getenv("SKG_CKPT");
+    ckpt_on_ = !(ck && std::atoi(ck) == 0) && ckpt_ && cap_ckpt_ >= (size_t)npool;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(s, &cs);
     timed_ = timing && cs == cudaStreamCaptureStatusNone;
@@ -1236,7 +1345,7 @@ cudaError_t WaveRunner::enqueue_tail() {
     W.jobs = nullptr; W.jtau = nullptr; W.jL = nullptr; W.jcount = ctr_ + 8 * (b ^ 1);
     W.pjobs = jobs_[b]; W.pjtau = jtau_[b]; W.pjL = jL_[b];
     W.last_busy = ctr_ + 16;
-    W.freelist = nullptr; W.intlist = nullptr;
+    W.freelist = nullptr; W.intlist = nullptr; W.ckpt = ckpt_on_ ? ckpt_ : nullptr;
     cudaError_t e;
     if (timed_) {
         for (int i = 0; i < 2; i++)

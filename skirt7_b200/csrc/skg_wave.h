@@ -22,8 +22,9 @@ public:
     ~WaveRunner();
 
     // Sizes the pool and job buffers (allocates; call outside stream capture).  pool packets,
-    // ngroups peel-off groups at most per packet.
-    cudaError_t reserve(size_t pool, int ngroups);
+    // ngroups peel-off groups at most per packet; grid_type decides whether path walks keep
+    // checkpoints (grids whose FP32 walk resumes).
+    cudaError_t reserve(size_t pool, int ngroups, int grid_type);
     // Enqueues the reset of the pool and the first waves of a phase on stream s.  P holds the
     // staged tables; nslots the slots whose DevGrid the traversal pass keeps in shared memory;
     // tree_walk the FP32 tree walk (TreeWalk) of tree grids.
@@ -54,6 +55,8 @@ private:
     Packet* pk_ = nullptr;
     int* free_ = nullptr;             // [pool] records freed in a wave, [pool] records at their
                                       // interaction point (the scatter-and-launch pass's work)
+    float4* ckpt_ = nullptr;          // [pool][checkpoints][2] path-walk checkpoints
+    size_t cap_ckpt_ = 0;
     size_t cap_pool_ = 0;
     int2* jobs_[2] = {nullptr, nullptr};
     double* jtau_[2] = {nullptr, nullptr};
@@ -74,6 +77,7 @@ private:
     std::vector<cudaEvent_t> ev_;      // 3 per wave: before the event pass, between, after the traversal
     bool timed_ = false;               // the running phase records ev_
     int tail_div_ = 16;
+    bool ckpt_on_ = true;              // path-walk checkpoints (environment variable SKG_CKPT=0: off)
     bool tail_ran_ = false;            // the phase ended with the tail pass
     cudaEvent_t tail_ev_[2] = {nullptr, nullptr};
 };

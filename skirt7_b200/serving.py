@@ -104,11 +104,14 @@ class Server:
         self.peak_resident = 0
         self.peak_in_use = 0
         self.ticks = 0
+        self.tick_gpu_s = 0.0        # device time of the ticks (CUDA events around each launch)
+        self.admit_s = 0.0           # host time spent admitting (model and context set-up)
 
     def close(self):
         self.batch.close()
 
     def _admit(self, req, now):
+        t0 = time.perf_counter()
         m = build_model(req, self.npix)
         ctx = runtime.Context(m, device=self.device)
         req._ctx = ctx
@@ -120,6 +123,7 @@ class Server:
         self.resident += 1
         self.peak_resident = max(self.peak_resident, self.resident)
         self.peak_in_use = max(self.peak_in_use, self.in_use)
+        self.admit_s += time.perf_counter() - t0
 
     def _retire(self, req, now):
         ctx = req._ctx
@@ -177,6 +181,7 @@ class Server:
             # arrivals are admitted (contexts built on their own streams) while the tick runs
             admit(time.perf_counter() - t0, len(active))
             self.batch.sync()
+            self.tick_gpu_s += self.batch.last_ms() / 1e3
             self.ticks += 1
             now = time.perf_counter() - t0
             still = []
