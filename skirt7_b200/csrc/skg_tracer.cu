@@ -106,12 +106,14 @@ namespace skg {
 #define SKG_CKPT 1
 #endif
 // cell steps a lane takes per pass of the traversal loop (the warp's refill and end-of-path votes
-// run once per pass): peel-off-job kernel, path-job kernel
+// run once per pass): peel-off-job kernel, path-job kernel.  Traversal pass of a 10^7-packet
+// phase (octree disk / Cartesian disk): 1 and 1: 161 / 69.1 ms; 2 and 1: 156 / 68.6; 2 and 2: 153 /
+// 68.1; 2 and 3: 152.5 / 66.9; 3 or 4 steps in the peel-off kernel spill: 165 / 68.3
 #ifndef SKG_INNER_STEPS
-#define SKG_INNER_STEPS 1
+#define SKG_INNER_STEPS 2
 #endif
 #ifndef SKG_INNER_PATH
-#define SKG_INNER_PATH 1
+#define SKG_INNER_PATH 3
 #endif
 #ifndef SKG_CKPT_N
 #define SKG_CKPT_N 32
@@ -140,8 +142,11 @@ template<typename R> SKG_D double kappa_rho(const DevScene& S, int m, int ell) {
 // FullInstrument.cpp:109-177).  SED bins go to the block's private copy `psed` when it is given
 // (every packet of a wavelength adds to the same SED bin: global atomics would serialise on it).
 // Returns the number of tally updates.
+// detect_group inlined into the event kernel: its call kept a 240-byte stack frame there (972
+// bytes of spill loads per thread at 64 registers against 52 inlined); event pass of a
+// 10^7-packet phase 14.3 against 16.1 ms (octree disk)
 #ifndef SKG_DETECT_INLINE
-#define SKG_DETECT_INLINE 0
+#define SKG_DETECT_INLINE 1
 #endif
 #if SKG_DETECT_INLINE
 __device__ __forceinline__
