@@ -17,7 +17,9 @@ the request's seed and the packet's index), so its result is the same alone and 
 to the summation order of the FP64 tally atomics.
 """
 import math
+import threading
 import time
+from concurrent.futures import Future, ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -83,10 +85,12 @@ class Server:
                  tick_budget packets (all wavelengths) are given out, so the oldest requests finish
                  first and the longest wait -- the p99 latency of a loaded loop -- is shortest;
                  "share": every admitted request runs a slice every tick (processor sharing)
+    threads      build the contexts of admitted requests, and read and release those of retired
+                 ones, on two host threads while the ticks run (False: between ticks)
     """
 
     def __init__(self, device=0, hbm_budget=40 << 30, max_slots=64, tick_packets=1 << 20, npix=256,
-                 precision=A.PREC_FP32, policy="fifo", tick_budget=6 << 20):
+                 precision=A.PREC_FP32, policy="fifo", tick_budget=6 << 20, threads=True):
         self.device = device
         self.budget = hbm_budget
         self.max_slots = max_slots
@@ -101,105 +105,162 @@ class Server:
         self.reserved = 0            # footprint bounds of the resident contexts (admission)
         self.in_use = 0              # their actual device bytes
         self.resident = 0            # resident contexts
+        self.held = 0                # admitted requests whose reservation is not released yet
+        self.peak_held = 0
         self.peak_resident = 0
         self.peak_in_use = 0
         self.ticks = 0
         self.tick_gpu_s = 0.0        # device time of the ticks (CUDA events around each launch)
         self.admit_s = 0.0           # host time spent admitting (model and context set-up)
+        self.threads = threads
+        self._lock = threading.Lock()   # the counters above, shared with the set-up threads
 
     def close(self):
         self.batch.close()
 
-    def _admit(self, req, now):
+    def _admit(self, req):
+        """Builds the request's model and context (its footprint is reserved already)."""
         t0 = time.perf_counter()
         m = build_model(req, self.npix)
         ctx = runtime.Context(m, device=self.device)
         req._ctx = ctx
         req._next = 0
-        req.admitted = now
-        req._reserved = _footprint(req, self.npix)
-        self.reserved += req._reserved
-        self.in_use += ctx.device_bytes
-        self.resident += 1
-        self.peak_resident = max(self.peak_resident, self.resident)
-        self.peak_in_use = max(self.peak_in_use, self.in_use)
-        self.admit_s += time.perf_counter() - t0
+        with self._lock:
+            self.in_use += ctx.device_bytes
+            self.resident += 1
+            self.peak_resident = max(self.peak_resident, self.resident)
+            self.peak_in_use = max(self.peak_in_use, self.in_use)
+            self.admit_s += time.perf_counter() - t0
 
-    def _retire(self, req, now):
+    def _retire(self, req, t0):
+        """Reads the request's frame (its result, at which its latency ends) and frees its context
+        and reservation."""
         ctx = req._ctx
         cube, _ = ctx.read_instrument(0)
         req.frame = cube[0]
-        req.done = now
-        self.in_use -= ctx.device_bytes
-        self.reserved -= req._reserved
-        self.resident -= 1
+        req.done = time.perf_counter() - t0
+        nbytes = ctx.device_bytes
         ctx.close()
         req._ctx = None
+        with self._lock:
+            self.in_use -= nbytes
+            self.reserved -= req._reserved
+            self.held -= 1
+            self.resident -= 1
 
     def serve(self, requests, realtime=True, on_tick=None):
         """Runs the request stream to completion; returns the requests with their results and
         timings.  realtime: arrivals follow the wall clock (else all are present at t=0)."""
         pending = sorted(requests, key=lambda r: r.arrival)
         active = []          # in the running tick
-        joining = []         # admitted while a tick runs: they join the next one
+        building = []        # (request, future): admitted, context being built
+        releasing = []       # futures of retired requests' frame reads and releases
         finished = []
         t0 = time.perf_counter()
         i = 0
+        if self.threads:
+            setup, release = ThreadPoolExecutor(max_workers=1), ThreadPoolExecutor(max_workers=1)
+        else:
+            setup = release = _Inline()
 
         def admit(now, n_on_device):
             nonlocal i
             while i < len(pending) and (not realtime or pending[i].arrival <= now) and n_on_device < self.max_slots:
-                if n_on_device and self.reserved + _footprint(pending[i], self.npix) > self.budget:
-                    break
-                self._admit(pending[i], now)
-                joining.append(pending[i])
+                fp = _footprint(pending[i], self.npix)
+                # (contexts still being released hold their reservations)
+                held = n_on_device or any(not f.done() for f in releasing)
+                with self._lock:
+                    if held and self.reserved + fp > self.budget:
+                        break
+                    self.reserved += fp
+                    self.held += 1
+                    self.peak_held = max(self.peak_held, self.held)
+                r = pending[i]
+                r._reserved = fp
+                r.admitted = now
+                building.append((r, setup.submit(self._admit, r)))
                 n_on_device += 1
                 i += 1
 
-        while i < len(pending) or active or joining:
-            active += joining
-            joining.clear()
-            if not active:
-                now = time.perf_counter() - t0
-                admit(now, 0)
-                if not joining and i < len(pending):
-                    time.sleep(max(0.0, min(0.01, pending[i].arrival - now)))
-                continue
-            # one tick: the next slice of the admitted requests in one batched launch
-            slices, given = [], {}
-            budget = self.tick_budget
-            for r in sorted(active, key=lambda q: q.arrival):
-                cnt = min(self.tick_packets, r.packets - r._next)
-                if self.policy == "fifo":
-                    if budget <= 0:
-                        break
-                    cnt = max(1, min(cnt, budget // 3))
-                    budget -= 3 * cnt
-                slices.append((r._ctx, [0, 1, 2], r.packets, r._next, cnt, r.seed))
-                given[r.rid] = cnt
-            self.batch.run(A.PHASE_STELLAR, slices, precision=self.precision)
-            # arrivals are admitted (contexts built on their own streams) while the tick runs
-            admit(time.perf_counter() - t0, len(active))
-            self.batch.sync()
-            self.tick_gpu_s += self.batch.last_ms() / 1e3
-            self.ticks += 1
-            now = time.perf_counter() - t0
-            still = []
-            for r in active:
-                if r.rid not in given:
-                    still.append(r)
+        def joined():
+            """Requests whose context is built (in admission order)."""
+            out = []
+            while building and building[0][1].done():
+                r, f = building.pop(0)
+                f.result()
+                out.append(r)
+            return out
+
+        try:
+            while i < len(pending) or active or building:
+                active += joined()
+                if not active:
+                    now = time.perf_counter() - t0
+                    admit(now, len(building))
+                    if building:
+                        building[0][1].result()          # wait for the first context
+                    elif i < len(pending) and (not realtime or pending[i].arrival <= now):
+                        for f in releasing:              # due, but over the budget: wait for a release
+                            if not f.done():
+                                f.result()
+                                break
+                    elif i < len(pending):
+                        time.sleep(max(0.0, min(0.01, pending[i].arrival - now)))
                     continue
-                r._next += given[r.rid]
-                r.ticks += 1
-                if r._next >= r.packets:
-                    self._retire(r, time.perf_counter() - t0)
-                    finished.append(r)
-                else:
-                    still.append(r)
-            active = still
-            if on_tick:
-                on_tick(self, now)
+                # one tick: the next slice of the admitted requests in one batched launch
+                slices, given = [], {}
+                budget = self.tick_budget
+                for r in sorted(active, key=lambda q: q.arrival):
+                    cnt = min(self.tick_packets, r.packets - r._next)
+                    if self.policy == "fifo":
+                        if budget <= 0:
+                            break
+                        cnt = max(1, min(cnt, budget // 3))
+                        budget -= 3 * cnt
+                    slices.append((r._ctx, [0, 1, 2], r.packets, r._next, cnt, r.seed))
+                    given[r.rid] = cnt
+                self.batch.run(A.PHASE_STELLAR, slices, precision=self.precision)
+                # arrivals are admitted while the tick runs: their contexts are built (on their own
+                # streams) by the set-up thread and join a later tick
+                admit(time.perf_counter() - t0, len(active) + len(building))
+                self.batch.sync()
+                self.tick_gpu_s += self.batch.last_ms() / 1e3
+                self.ticks += 1
+                now = time.perf_counter() - t0
+                still = []
+                for r in active:
+                    if r.rid not in given:
+                        still.append(r)
+                        continue
+                    r._next += given[r.rid]
+                    r.ticks += 1
+                    if r._next >= r.packets:
+                        finished.append(r)
+                        releasing.append(release.submit(self._retire, r, t0))
+                    else:
+                        still.append(r)
+                active = still
+                if on_tick:
+                    on_tick(self, now)
+            for f in releasing:
+                f.result()
+        finally:
+            if self.threads:
+                setup.shutdown(wait=True)
+                release.shutdown(wait=True)
         return finished
+
+
+class _Inline:
+    """An executor that runs each call at once (Server(threads=False))."""
+
+    def submit(self, fn, *args):
+        f = Future()
+        try:
+            f.set_result(fn(*args))
+        except BaseException as e:   # surfaced by f.result(), as a thread pool does
+            f.set_exception(e)
+        return f
 
 
 def _footprint(req, npix):

@@ -34,9 +34,16 @@ def test_admission_by_memory_budget():
     done = srv.serve(reqs, realtime=False)
     srv.close()
     assert len(done) == len(reqs)
-    # two 48^3 variants fit the budget, three do not; the bound holds for the real footprint
-    assert srv.peak_resident == 2
+    # two 48^3 variants fit the budget, three do not (admitted requests hold their reservation
+    # until their context is released); the bound holds for the real footprint
+    assert srv.peak_held == 2 and srv.peak_resident <= 2
     assert srv.peak_in_use <= 2 * est <= srv.budget
+    # the same with contexts built and released between ticks
+    srv = serving.Server(max_slots=8, tick_packets=1 << 20, npix=64, hbm_budget=int(2.5 * est), threads=False)
+    done = srv.serve(serving.fitskirt_requests(n=6, rate=0.0, seed=8, packets=(2e4, 4e4), grid=(48, 48)),
+                     realtime=False)
+    srv.close()
+    assert len(done) == 6 and srv.peak_held == 2 and srv.peak_resident == 2
 
 
 def test_fifo_policy_serves_the_oldest_first():
