@@ -52,7 +52,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--tree-cache", default=os.path.join(ROOT, ".bench_cache", "octree.npz"),
                    help="cache of the headline octree between runs of the same size (git-ignored)")
-    p.add_argument("--serving", type=int, default=64,
+    p.add_argument("--serving", type=int, default=256,
                    help="requests of the fit-variant serving leg (Poisson 20/s; 0 = skip)")
     return p.parse_args()
 

@@ -46,6 +46,7 @@ class Request:
     frame: np.ndarray = None
     _ctx: object = field(default=None, repr=False)
     _next: int = 0                 # first packet of the next slice
+    _ran: int = 0                  # packets whose ticks have completed
     _reserved: int = 0             # device bytes reserved at admission
 
     @property
@@ -87,10 +88,13 @@ class Server:
                  "share": every admitted request runs a slice every tick (processor sharing)
     threads      build the contexts of admitted requests, and read and release those of retired
                  ones, on two host threads while the ticks run (False: between ticks)
+    pipeline     ticks in flight at once (each on a batch of its own): the next tick is launched
+                 while the previous one drains its last packets (2 measured no faster than 1 on
+                 the fit-variant stream: the device is busy either way)
     """
 
     def __init__(self, device=0, hbm_budget=40 << 30, max_slots=64, tick_packets=1 << 20, npix=256,
-                 precision=A.PREC_FP32, policy="fifo", tick_budget=6 << 20, threads=True):
+                 precision=A.PREC_FP32, policy="fifo", tick_budget=6 << 20, threads=True, pipeline=1):
         self.device = device
         self.budget = hbm_budget
         self.max_slots = max_slots
@@ -101,7 +105,9 @@ class Server:
             raise ValueError("policy is 'fifo' or 'share'")
         self.policy = policy
         self.tick_budget = int(tick_budget)
-        self.batch = runtime.Batch(device=device, max_slots=max_slots, max_items=max_slots, max_ells=3 * max_slots)
+        self.batches = [runtime.Batch(device=device, max_slots=max_slots, max_items=max_slots, max_ells=3 * max_slots)
+                        for _ in range(max(1, int(pipeline)))]
+        self.batch = self.batches[0]
         self.reserved = 0            # footprint bounds of the resident contexts (admission)
         self.in_use = 0              # their actual device bytes
         self.resident = 0            # resident contexts
@@ -110,13 +116,14 @@ class Server:
         self.peak_resident = 0
         self.peak_in_use = 0
         self.ticks = 0
-        self.tick_gpu_s = 0.0        # device time of the ticks (CUDA events around each launch)
+        self.tick_gpu_s = 0.0        # device time of the ticks, summed (CUDA events around each launch)
         self.admit_s = 0.0           # host time spent admitting (model and context set-up)
         self.threads = threads
         self._lock = threading.Lock()   # the counters above, shared with the set-up threads
 
     def close(self):
-        self.batch.close()
+        for b in self.batches:
+            b.close()
 
     def _admit(self, req):
         """Builds the request's model and context (its footprint is reserved already)."""
@@ -125,6 +132,7 @@ class Server:
         ctx = runtime.Context(m, device=self.device)
         req._ctx = ctx
         req._next = 0
+        req._ran = 0
         with self._lock:
             self.in_use += ctx.device_bytes
             self.resident += 1
@@ -191,57 +199,63 @@ class Server:
                 out.append(r)
             return out
 
+        inflight = []        # (batch, [(request, packets)]): launched ticks, oldest first
+        free = list(self.batches)
         try:
-            while i < len(pending) or active or building:
+            while i < len(pending) or active or building or inflight:
                 active += joined()
-                if not active:
-                    now = time.perf_counter() - t0
-                    admit(now, len(building))
-                    if building:
-                        building[0][1].result()          # wait for the first context
-                    elif i < len(pending) and (not realtime or pending[i].arrival <= now):
-                        for f in releasing:              # due, but over the budget: wait for a release
-                            if not f.done():
-                                f.result()
+                waiting = [r for r in active if r._next < r.packets]
+                if waiting and free:
+                    # one tick: the next slices of the admitted requests in one batched launch
+                    slices, given = [], []
+                    budget = self.tick_budget
+                    for r in sorted(waiting, key=lambda q: q.arrival):
+                        cnt = min(self.tick_packets, r.packets - r._next)
+                        if self.policy == "fifo":
+                            if budget <= 0:
                                 break
-                    elif i < len(pending):
-                        time.sleep(max(0.0, min(0.01, pending[i].arrival - now)))
+                            cnt = max(1, min(cnt, budget // 3))
+                            budget -= 3 * cnt
+                        slices.append((r._ctx, [0, 1, 2], r.packets, r._next, cnt, r.seed))
+                        given.append((r, cnt))
+                        r._next += cnt
+                    b = free.pop(0)
+                    b.run(A.PHASE_STELLAR, slices, precision=self.precision)
+                    inflight.append((b, given))
+                    # arrivals are admitted while ticks run: their contexts are built (on their own
+                    # streams) by the set-up thread and join a later tick
+                    admit(time.perf_counter() - t0, len(active) + len(building))
                     continue
-                # one tick: the next slice of the admitted requests in one batched launch
-                slices, given = [], {}
-                budget = self.tick_budget
-                for r in sorted(active, key=lambda q: q.arrival):
-                    cnt = min(self.tick_packets, r.packets - r._next)
-                    if self.policy == "fifo":
-                        if budget <= 0:
-                            break
-                        cnt = max(1, min(cnt, budget // 3))
-                        budget -= 3 * cnt
-                    slices.append((r._ctx, [0, 1, 2], r.packets, r._next, cnt, r.seed))
-                    given[r.rid] = cnt
-                self.batch.run(A.PHASE_STELLAR, slices, precision=self.precision)
-                # arrivals are admitted while the tick runs: their contexts are built (on their own
-                # streams) by the set-up thread and join a later tick
-                admit(time.perf_counter() - t0, len(active) + len(building))
-                self.batch.sync()
-                self.tick_gpu_s += self.batch.last_ms() / 1e3
-                self.ticks += 1
+                if inflight:
+                    admit(time.perf_counter() - t0, len(active) + len(building))
+                    b, given = inflight.pop(0)
+                    b.sync()
+                    self.tick_gpu_s += b.last_ms() / 1e3
+                    self.ticks += 1
+                    free.append(b)
+                    now = time.perf_counter() - t0
+                    for r, cnt in given:
+                        r._ran += cnt
+                        r.ticks += 1
+                        if r._ran >= r.packets:
+                            finished.append(r)
+                            releasing.append(release.submit(self._retire, r, t0))
+                    active = [r for r in active if r._ran < r.packets]
+                    if on_tick:
+                        on_tick(self, now)
+                    continue
+                # nothing on the device and nothing admitted
                 now = time.perf_counter() - t0
-                still = []
-                for r in active:
-                    if r.rid not in given:
-                        still.append(r)
-                        continue
-                    r._next += given[r.rid]
-                    r.ticks += 1
-                    if r._next >= r.packets:
-                        finished.append(r)
-                        releasing.append(release.submit(self._retire, r, t0))
-                    else:
-                        still.append(r)
-                active = still
-                if on_tick:
-                    on_tick(self, now)
+                admit(now, len(building))
+                if building:
+                    building[0][1].result()          # wait for the first context
+                elif i < len(pending) and (not realtime or pending[i].arrival <= now):
+                    for f in releasing:              # due, but over the budget: wait for a release
+                        if not f.done():
+                            f.result()
+                            break
+                elif i < len(pending):
+                    time.sleep(max(0.0, min(0.01, pending[i].arrival - now)))
             for f in releasing:
                 f.result()
         finally:

@@ -59,3 +59,16 @@ def test_fifo_policy_serves_the_oldest_first():
     for r in done[:2]:
         alone, _ = serving.run_alone(r, npix=64)
         assert np.allclose(r.frame, alone, rtol=1e-10, atol=1e-12 * alone.max()), r.rid
+
+
+def test_pipelined_ticks_give_the_same_results():
+    """Two ticks in flight at once (each on its own batch; a request's slices can run in both):
+    every frame is still the one the request gives alone, and requests retire in tick order."""
+    reqs = serving.fitskirt_requests(n=6, rate=0.0, seed=10, packets=(2e4, 1e5), grid=(24, 32))
+    srv = serving.Server(max_slots=6, tick_packets=20000, npix=64, pipeline=2, tick_budget=3 * 40000)
+    done = srv.serve(reqs, realtime=False)
+    srv.close()
+    assert len(done) == len(reqs) and any(r.ticks > 1 for r in done)
+    for r in done[:3]:
+        alone, _ = serving.run_alone(r, npix=64)
+        assert np.allclose(r.frame, alone, rtol=1e-10, atol=1e-12 * alone.max()), r.rid
