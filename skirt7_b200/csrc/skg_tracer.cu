@@ -109,6 +109,11 @@ namespace skg {
 // run once per pass): peel-off-job kernel, path-job kernel.  Traversal pass of a 10^7-packet
 // phase (octree disk / Cartesian disk): 1 and 1: 161 / 69.1 ms; 2 and 1: 156 / 68.6; 2 and 2: 153 /
 // 68.1; 2 and 3: 152.5 / 66.9; 3 or 4 steps in the peel-off kernel spill: 165 / 68.3
+// the scatter-and-launch pass's grid: the blocks resident at once (1), or 16 per SM (0);
+// event + launch passes of a 10^7-packet octree-disk phase 13.3 against 14.4 ms
+#ifndef SKG_LAUNCH_OCC
+#define SKG_LAUNCH_OCC 1
+#endif
 #ifndef SKG_INNER_STEPS
 #define SKG_INNER_STEPS 2
 #endif
@@ -1172,13 +1177,18 @@ cudaError_t enqueue_wave(const WaveParams& W, int nslots, int trav_blocks, cudaE
     event_kernel<R><<<(W.npool + SKG_EVENT_THREADS - 1) / SKG_EVENT_THREADS, SKG_EVENT_THREADS, 0, s>>>(W);
 #if SKG_LAUNCH_KERNEL
     {
-        static int sms = 0;
+        // a grid-stride pass: SKG_LAUNCH_OCC sizes it to the blocks that are resident at once
+        static int sms = 0, per = 16;
         if (sms == 0) {
             int dev = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+#if SKG_LAUNCH_OCC
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, launch_kernel<R>, SKG_EVENT_THREADS, 0);
+            if (per <= 0) per = 1;
+#endif
         }
-        launch_kernel<R><<<sms * 16, SKG_EVENT_THREADS, 0, s>>>(W);
+        launch_kernel<R><<<sms * per, SKG_EVENT_THREADS, 0, s>>>(W);
     }
 #endif
     if (mid) cudaEventRecord(mid, s);
