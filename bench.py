@@ -395,6 +395,10 @@ def main():
 
     # ---- end to end through the C ABI with host buffers: reset, run, read the frames to host
     cubes_bytes = 8 * sum(sizes)
+    # page-locked host arrays for the frames, allocated once and reused every step (as a caller
+    # keeps its output images)
+    host = [torch.empty(n, dtype=torch.float64, pin_memory=True) for n in sizes]
+    host_out = {i: (h.numpy(), np.empty(_tally_len(ctx, i, sed=True))) for i, h in zip(fr, host)}
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -405,12 +409,13 @@ def main():
             ctx.sync()
             step(3000 + 10 * s)
             if rank == 0:
-                host = [t.cpu() for t in red]      # the reduced frames, device -> host
+                for h, t in zip(host, red):        # the reduced frames, device -> host
+                    h.copy_(t)
             torch.cuda.synchronize()
         else:
             run_phases(3000 + 10 * s, None)
             for i in fr:
-                ctx.read_instrument(i)             # synchronises, then device -> host
+                ctx.read_instrument(i, out=host_out[i])   # synchronises, then device -> host
     e2e_s = time.perf_counter() - t0
     if dist:
         t = torch.tensor([e2e_s], device="cuda")
@@ -460,11 +465,11 @@ def main():
         dist.destroy_process_group()
 
 
-def _tally_len(ctx, i):
+def _tally_len(ctx, i, sed=False):
     import ctypes as C
     cl, sl = C.c_int64(), C.c_int64()
     ctx.lib.skg_tally_sizes(ctx.h, i, C.byref(cl), C.byref(sl))
-    return cl.value
+    return sl.value if sed else cl.value
 
 
 def serving_leg(args, device):

@@ -119,15 +119,24 @@ class Context:
     def reset_tallies(self):
         self._ck(self.lib.skg_reset_tallies(self.h))
 
-    def read_instrument(self, i):
+    def read_instrument(self, i, out=None):
         """(cube, sed): cube shaped [components, nlambda, nyp, nxp] (None for SED instruments),
-        sed shaped [components, nlambda]."""
+        sed shaped [components, nlambda].  out: (cube, sed) flat float64 host arrays of the
+        instrument's tally sizes to read into (e.g. page-locked buffers reused every step)."""
         cl, sl = C.c_int64(), C.c_int64()
         self._ck(self.lib.skg_tally_sizes(self.h, i, C.byref(cl), C.byref(sl)))
         ins = self.model.instruments[i]
         ncomp = sl.value // self.nlambda
-        sed = np.zeros(sl.value)
-        cube = np.zeros(cl.value) if cl.value else None
+        if out is not None:
+            cube, sed = out
+            if sed is None or sed.dtype != np.float64 or not sed.flags.c_contiguous or sed.size != sl.value or \
+                    (cl.value and (cube is None or cube.dtype != np.float64 or not cube.flags.c_contiguous or
+                                   cube.size != cl.value)):
+                raise ValueError("out: flat contiguous float64 arrays of the instrument's tally sizes")
+            cube = cube if cl.value else None
+        else:
+            sed = np.zeros(sl.value)
+            cube = np.zeros(cl.value) if cl.value else None
         self._ck(self.lib.skg_read_instrument(self.h, i, cube.ctypes.data_as(A.dp) if cube is not None else None,
                                               sed.ctypes.data_as(A.dp)))
         sed = sed.reshape(ncomp, self.nlambda)

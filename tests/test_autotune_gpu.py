@@ -27,6 +27,10 @@ def test_pool_and_blocks_do_not_change_results():
         assert waves > 1 and tr > 0 and ev > 0
     for f in frames[1:]:
         assert np.allclose(f, frames[0], rtol=1e-11, atol=1e-13 * frames[0].max())
+    # reading into caller-owned host arrays gives the same tallies
+    cube, sed = ctx.read_instrument(0)
+    c2, s2 = ctx.read_instrument(0, out=(np.empty(cube.size), np.empty(sed.size)))
+    assert np.array_equal(c2, cube) and np.array_equal(s2, sed)
     res = autotune.tune(ctx, A.PHASE_STELLAR, [0], 60000, sample=20000, pools=[1 << 12, 1 << 14], blocks=[148, 296])
     assert res["pool"] in (1 << 12, 1 << 14) and res["blocks"] in (148, 296) and len(res["trials"]) == 4
     assert autotune.tune(ctx, A.PHASE_STELLAR, [0], 60000) is res          # cached per workload class
