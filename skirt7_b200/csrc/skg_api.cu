@@ -20,15 +20,26 @@ using namespace skg;
 
 namespace {
 
+// Device allocations of one owner.  With a stream set they are stream-ordered (cudaMallocAsync /
+// cudaFreeAsync on that stream): releasing a context then does not synchronise the device, which
+// a plain cudaFree does -- a serving loop frees retired contexts while other simulations run.  The
+// owner synchronises the stream before another stream uses the memory.
 struct Allocs {
     std::vector<void*> ptrs;
     size_t bytes = 0;
+    cudaStream_t stream = nullptr;
     ~Allocs() { release(); }
-    void release() { for (void* p : ptrs) cudaFree(p); ptrs.clear(); bytes = 0; }
+    void release() {
+        for (void* p : ptrs) {
+            if (stream) cudaFreeAsync(p, stream); else cudaFree(p);
+        }
+        ptrs.clear(); bytes = 0;
+    }
     template<typename T> T* alloc(size_t n) {
         if (n == 0) n = 1;
         void* p = nullptr;
-        if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+        const cudaError_t e = stream ? cudaMallocAsync(&p, n * sizeof(T), stream) : cudaMalloc(&p, n * sizeof(T));
+        if (e != cudaSuccess) { cudaGetLastError(); return nullptr; }
         ptrs.push_back(p); bytes += n * sizeof(T);
         return (T*)p;
     }
@@ -396,6 +407,7 @@ int skg_ctx_create(const skg_scene* sc, int device, skg_ctx** out) {
         ctx->waves.timing = true;
         cudaStream_t s = ctx->stream;
         Allocs& A = ctx->A;
+        A.stream = s;                      // stream-ordered; the stream is synchronised below
 
         REQUIRE(sc->nlambda > 0 && sc->lambda && sc->dlambda, "wavelength grid is empty");
         REQUIRE(sc->ncomp >= 0 && sc->ncomp <= MAX_COMP, "at most 4 dust components");

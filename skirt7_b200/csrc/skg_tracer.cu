@@ -1251,11 +1251,10 @@ PassFns pick(int grid_type, int tree_walk, int precision) {
 WaveRunner::~WaveRunner() {
     for (cudaEvent_t e : ev_) cudaEventDestroy(e);
     for (cudaEvent_t e : tail_ev_) if (e) cudaEventDestroy(e);
-    cudaFree(pk_);
-    cudaFree(free_);
-    cudaFree(ckpt_);
-    for (int b = 0; b < 2; b++) { cudaFree(jobs_[b]); cudaFree(jtau_[b]); cudaFree(jL_[b]); }
-    cudaFree(ctr_);
+    // (a runner that never reserved frees nothing: no device-wide synchronisation)
+    for (void* p : {(void*)pk_, (void*)free_, (void*)ckpt_, (void*)ctr_}) if (p) cudaFree(p);
+    for (int b = 0; b < 2; b++)
+        for (void* p : {(void*)jobs_[b], (void*)jtau_[b], (void*)jL_[b]}) if (p) cudaFree(p);
     if (h_ctr_) cudaFreeHost(h_ctr_);
     if (copied_) cudaEventDestroy(copied_);
 }
