@@ -480,7 +480,7 @@ def serving_leg(args, device):
     import numpy as np
     from skirt7_b200 import serving
     reqs = serving.fitskirt_requests(n=args.serving, rate=20.0, seed=2024)
-    srv = serving.Server(device=device, max_slots=64, tick_packets=1 << 19, npix=256)
+    srv = serving.Server(device=device, max_slots=64, npix=256)
     t0 = time.perf_counter()
     done = srv.serve(reqs, realtime=True)
     wall = time.perf_counter() - t0

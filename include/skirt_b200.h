@@ -247,6 +247,9 @@ int         skg_device_count(int* count);
    device), mix tables, source samplers, instrument frames.  Replaces Simulation::setup
    (SimulationItem.cpp:18-31) for the items on the hot path. */
 int  skg_ctx_create(const skg_scene* scene, int device, skg_ctx** out);
+/* Waits for the context's own work and frees it.  Its device memory is stream-ordered (allocated
+   and freed on the context's stream, from the device's default memory pool), so destroying a
+   context does not synchronise the device: other contexts and batches keep running. */
 int  skg_ctx_destroy(skg_ctx* ctx);
 /* Number of dust cells, and the device bytes held by the context (admission by footprint). */
 int  skg_ctx_info(const skg_ctx* ctx, int64_t* ncells, int64_t* device_bytes);
