@@ -105,20 +105,21 @@ namespace skg {
 #ifndef SKG_CKPT
 #define SKG_CKPT 1
 #endif
-// cell steps a lane takes per pass of the traversal loop (the warp's refill and end-of-path votes
-// run once per pass): peel-off-job kernel, path-job kernel.  Traversal pass of a 10^7-packet
-// phase (octree disk / Cartesian disk): 1 and 1: 161 / 69.1 ms; 2 and 1: 156 / 68.6; 2 and 2: 153 /
-// 68.1; 2 and 3: 152.5 / 66.9; 3 or 4 steps in the peel-off kernel spill: 165 / 68.3
 // the scatter-and-launch pass's grid: the blocks resident at once (1), or 16 per SM (0);
 // event + launch passes of a 10^7-packet octree-disk phase 13.3 against 14.4 ms
 #ifndef SKG_LAUNCH_OCC
 #define SKG_LAUNCH_OCC 1
 #endif
+// cell steps a lane takes per pass of the traversal loop (the warp's refill and end-of-path votes
+// run once per pass): peel-off-job kernel, path-job kernel.  Traversal pass of a 10^7-packet
+// phase (octree disk / Cartesian disk): 1 and 1: 161 / 69.1 ms; 2 and 1: 156 / 68.6; 2 and 2: 153 /
+// 68.1; 2 and 3: 152.4 / 67.0; 2 and 4: 151.3 / 66.4; 3 or 4 steps in the peel-off kernel spill:
+// 165 / 68.3
 #ifndef SKG_INNER_STEPS
 #define SKG_INNER_STEPS 2
 #endif
 #ifndef SKG_INNER_PATH
-#define SKG_INNER_PATH 3
+#define SKG_INNER_PATH 4
 #endif
 #ifndef SKG_CKPT_N
 #define SKG_CKPT_N 32
