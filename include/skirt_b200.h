@@ -261,7 +261,8 @@ int  skg_read_density(skg_ctx* ctx, double* rho);
 /* For n rays (r[3n], k[3n]) computes the path through the grid exactly as DustGrid::path:
    cells[] and ds[] receive the segments of ray i at offsets[i] .. offsets[i+1]-1
    (m = -1 for segments outside the grid).  capacity = length of cells/ds.  Returns
-   SKG_ERR_CAPACITY (and the needed total in offsets[n]) when the buffers are too small. */
+   SKG_ERR_CAPACITY (and the needed total in offsets[n]) when the buffers are too small,
+   SKG_ERR_INVALID for a precision other than SKG_PREC_FP32 / SKG_PREC_FP64.  Synchronous. */
 int  skg_trace_paths(skg_ctx* ctx, const double* r, const double* k, int64_t n, int precision,
                      int32_t* cells, double* ds, int64_t* offsets, int64_t capacity);
 
@@ -274,10 +275,15 @@ int  skg_trace_paths(skg_ctx* ctx, const double* r, const double* k, int64_t n, 
    nothing: its scratch (per-ray counts and scan totals, 8 MiB + 8 KiB) is a static device array
    of this library, so n is limited to SKG_NOALLOC_MAX_RAYS (larger n returns SKG_ERR_CAPACITY
    at once).  The device address of that array is looked up on the first call on each device;
-   make that first call before any stream capture.  The work is enqueued on `stream` (NULL =
-   the context's stream) and the call returns without waiting; once that stream has completed,
-   skg_sync(ctx, ...) reports SKG_ERR_CAPACITY when the segments exceed `capacity` (d_offsets[n]
-   then holds the needed total) or SKG_ERR_STEP_BUDGET.  All calls on one device share the one
+   make that first call before any stream capture.  A phase still running on the context is
+   finished first (as every other entry point does).  The work is enqueued on `stream` (NULL =
+   the context's stream) and the call returns without waiting.  skg_sync(ctx, ...) waits for
+   the end of this work on that stream (bounded by its timeout) and then reports, once,
+   SKG_ERR_CAPACITY when the segments exceed `capacity` (d_offsets[n] then holds the needed
+   total) or SKG_ERR_STEP_BUDGET; a caller that does not call skg_sync can compare d_offsets[n]
+   with `capacity` itself.  These flags live in a word of the context that the phases do not
+   use, so the call never clears a finished phase's flags.  Any precision other than
+   SKG_PREC_FP32 / SKG_PREC_FP64 returns SKG_ERR_INVALID.  All calls on one device share the one
    scratch array: two calls whose work overlaps in time (different streams or threads, or
    different contexts on the same device) race and corrupt each other's results. */
 #define SKG_NOALLOC_MAX_RAYS 1048576
@@ -351,7 +357,11 @@ int  skg_read_instrument_device(skg_ctx* ctx, int instr, double* d_cube, double*
 /* Absorbed luminosity [ncells][nlambda] (stellar and dust parts separately; either may be NULL). */
 int  skg_read_absorption(skg_ctx* ctx, double* labs_stellar, double* labs_dust);
 int  skg_read_counters(skg_ctx* ctx, skg_counters* out);
-/* Synchronises the context stream with a bounded wait; SKG_ERR_TIMEOUT after timeout_ms. */
+/* Finishes the running phase and waits for the context stream (and for the last
+   skg_trace_paths_noalloc call on its caller's stream) with a bounded wait: SKG_ERR_TIMEOUT
+   after timeout_ms (-1 = no limit; a later call waits again).  Then reports the flags of the
+   last phase (SKG_ERR_NAN_TAU, SKG_ERR_STEP_BUDGET, SKG_ERR_CAPACITY; they stay until the next
+   phase starts) and of the last no-alloc path call (reported once). */
 int  skg_sync(skg_ctx* ctx, int timeout_ms);
 /* Device time (ms) of the last skg_run_phase launch (CUDA events on the launching stream). */
 int  skg_last_phase_ms(skg_ctx* ctx, float* ms);

@@ -1317,6 +1317,78 @@ static void sampleDensity(Sim& S, int Nrandom, int nthreads, uint64_t seed) {
     });
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// Tree construction: TreeDustGrid::setupSelfBefore / subdivide (TreeDustGrid.cpp:80-100,
+// 166-230) with the mass-fraction criterion, the node masses of TreeNodeSampleDensityCalculator
+// (TreeNodeSampleDensityCalculator.cpp:26-45: Nrandom positions uniform in the node box,
+// mass = mean density x volume), the total mass of DustComp::mass (DustComp.cpp:110-114: the
+// sum of the components' normalisations), and the children of OctTreeNode::createchildren
+// (OctTreeNode.cpp:38-56: eight boxes split at the centre) and BinTreeNode::createchildren
+// (BinTreeNode.cpp:40-77: two boxes split at the middle along direction level % 3).  Nodes are
+// visited in creation order; children are appended, so the ids follow the reference's.
+
+// Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11), restated to reproduce the library's
+// device sampler of node masses: key = seed, counter words = (block, node id lo, node id hi,
+// stream), deviates ((u32 + 0.5) * 2^-32).
+struct Philox {
+    uint32_t k0, k1, c1, c2, c3, c0 = 0, b[4]; int left = 0;
+    Philox(uint64_t seed, uint64_t id, uint32_t stream)
+        : k0((uint32_t)seed), k1((uint32_t)(seed >> 32)), c1((uint32_t)id), c2((uint32_t)(id >> 32)), c3(stream) {}
+    double uniform() {
+        if (left == 0) {
+            uint32_t x0 = c0, x1 = c1, x2 = c2, x3 = c3, a = k0, bb = k1;
+            for (int r = 0; r < 10; r++) {
+                uint64_t p0 = (uint64_t)0xD2511F53u * x0, p1 = (uint64_t)0xCD9E8D57u * x2;
+                uint32_t y0 = (uint32_t)(p1 >> 32) ^ x1 ^ a, y1 = (uint32_t)p1;
+                uint32_t y2 = (uint32_t)(p0 >> 32) ^ x3 ^ bb, y3 = (uint32_t)p0;
+                x0 = y0; x1 = y1; x2 = y2; x3 = y3;
+                a += 0x9E3779B9u; bb += 0xBB67AE85u;
+            }
+            b[0] = x0; b[1] = x1; b[2] = x2; b[3] = x3; left = 4; c0++;
+        }
+        return ((double)b[4 - (left--)] + 0.5) * 2.3283064365386963e-10;
+    }
+};
+
+struct TreeBuild {
+    vector<Box> box; vector<int> child, father, level; vector<int8_t> dir; vector<uint8_t> split;
+    void split_node(int l, int type) {
+        const Box b = box[l];
+        int id0 = (int)box.size();
+        child[l] = id0; split[l] = 1;
+        auto push = [&](const Box& c) {
+            box.push_back(c); child.push_back(-1); father.push_back(l); level.push_back(level[l] + 1);
+            dir.push_back(-1); split.push_back(0);
+        };
+        if (type == SKG_GRID_OCTREE) {                            // OctTreeNode.cpp:38-56
+            double xc = 0.5*(b.xmin+b.xmax), yc = 0.5*(b.ymin+b.ymax), zc = 0.5*(b.zmin+b.zmax);
+            push(Box{b.xmin, b.ymin, b.zmin, xc, yc, zc});
+            push(Box{xc, b.ymin, b.zmin, b.xmax, yc, zc});
+            push(Box{b.xmin, yc, b.zmin, xc, b.ymax, zc});
+            push(Box{xc, yc, b.zmin, b.xmax, b.ymax, zc});
+            push(Box{b.xmin, b.ymin, zc, xc, yc, b.zmax});
+            push(Box{xc, b.ymin, zc, b.xmax, yc, b.zmax});
+            push(Box{b.xmin, yc, zc, xc, b.ymax, b.zmax});
+            push(Box{xc, yc, zc, b.xmax, b.ymax, b.zmax});
+        } else {                                                   // BinTreeNode.cpp:40-77
+            int d = level[l] % 3;
+            dir[l] = (int8_t)d;
+            Box c0 = b, c1 = b;
+            if (d == 0) { double c = 0.5*(b.xmin+b.xmax); c0.xmax = c; c1.xmin = c; }
+            else if (d == 1) { double c = 0.5*(b.ymin+b.ymax); c0.ymax = c; c1.ymin = c; }
+            else { double c = 0.5*(b.zmin+b.zmax); c0.zmax = c; c1.zmin = c; }
+            push(c0); push(c1);
+        }
+    }
+};
+
+static double dust_density(const Sim& S, Vec r) {            // CompDustDistribution / DustComp::density
+    double rho = 0;
+    for (int h = 0; h < S.ncomp; h++) rho += S.dustnorm[h]*S.dustgeom[h].density(r);
+    return rho;
+}
+
 }  // namespace orc
 
 // =============================================================================================
@@ -1340,26 +1412,50 @@ int orc_chunk_params(double packages, int nthreads, int nprocs, int nlambda,
     return 0;
 }
 
-// DustGrid::path for n rays; segments of ray i at offsets[i]..offsets[i+1]-1.
+// DustGrid::path for n rays; segments of ray i at offsets[i]..offsets[i+1]-1.  The rays are
+// independent: nthreads threads trace contiguous ranges of them into per-range buffers, which are
+// then concatenated in ray order (the output does not depend on the thread count).
 int orc_trace_paths(const skg_scene* sc, const double* r, const double* k, int64_t n,
-                    int32_t* cells, double* ds, int64_t* offsets, int64_t capacity, int64_t* fallbacks) {
+                    int32_t* cells, double* ds, int64_t* offsets, int64_t capacity, int64_t* fallbacks,
+                    int nthreads) {
     Sim* S = buildSim(sc);
-    int64_t pos = 0; int rc = 0; long fb = 0;
-    Path p;
-    for (int64_t i = 0; i < n; i++) {
-        p.r = Vec(r[3*i], r[3*i+1], r[3*i+2]); p.k = Vec(k[3*i], k[3*i+1], k[3*i+2]);
-        S->grid->path(p, &fb);
-        offsets[i] = pos;
-        for (auto& s : p.v) {
-            if (pos < capacity) { cells[pos] = s.m; ds[pos] = s.ds; }
-            pos++;
+    if (nthreads < 1) nthreads = 1;
+    const int64_t nr = std::max<int64_t>(1, std::min<int64_t>(nthreads * 4, n));
+    struct Range { vector<int32_t> m; vector<double> d; vector<int64_t> cnt; long fb = 0; };
+    vector<Range> R(nr);
+    std::atomic<int64_t> next{0};
+    auto worker = [&]() {
+        Path p;
+        int64_t q;
+        while ((q = next.fetch_add(1)) < nr) {
+            Range& g = R[q];
+            const int64_t i0 = n*q/nr, i1 = n*(q+1)/nr;
+            for (int64_t i = i0; i < i1; i++) {
+                p.r = Vec(r[3*i], r[3*i+1], r[3*i+2]); p.k = Vec(k[3*i], k[3*i+1], k[3*i+2]);
+                S->grid->path(p, &g.fb);
+                g.cnt.push_back((int64_t)p.v.size());
+                for (auto& s : p.v) { g.m.push_back(s.m); g.d.push_back(s.ds); }
+            }
         }
+    };
+    vector<std::thread> th;
+    for (int t = 1; t < nthreads; t++) th.emplace_back(worker);
+    worker();
+    for (auto& t : th) t.join();
+    int64_t pos = 0, i = 0; long fb = 0;
+    for (auto& g : R) {
+        size_t j = 0;
+        for (int64_t c : g.cnt) {
+            offsets[i++] = pos;
+            for (int64_t e = 0; e < c; e++, j++, pos++)
+                if (pos < capacity) { cells[pos] = g.m[j]; ds[pos] = g.d[j]; }
+        }
+        fb += g.fb;
     }
     offsets[n] = pos;
-    if (pos > capacity) rc = SKG_ERR_CAPACITY;
     if (fallbacks) *fallbacks = fb;
     delete S->grid; delete S;
-    return rc;
+    return pos > capacity ? SKG_ERR_CAPACITY : 0;
 }
 
 // Instrument::opticalDepth for n rays at wavelength ell with the given densities.
@@ -1441,6 +1537,86 @@ int orc_sample_density(const skg_scene* sc, int nthreads, uint64_t seed, double*
     return 0;
 }
 
+
+// TreeDustGrid construction (see TreeBuild above).  sampler 0: the reference's Random::position
+// (Random.cpp:227-235) from one MT19937 stream seeded `seed`, node after node and sample after
+// sample (the order of a single-threaded run); sampler 1: one counter-based stream per node and
+// sample, the sampler of the library's device builder (identical node masses, so identical
+// decisions).  Writes, in node creation order, the split flags, boxes, first-child ids, fathers,
+// cell numbers (leaves in node order, TreeDustGrid.cpp:107-119; -1 otherwise), split directions
+// (k-d tree) and levels.  *nnodes receives the node count; SKG_ERR_CAPACITY when it exceeds
+// max_nodes (nothing else is written then).
+int orc_tree_build(const skg_scene* sc, int type, int minlevel, int maxlevel, double maxfrac, int Nrandom,
+                   uint64_t seed, int sampler, int nthreads, int64_t max_nodes, uint8_t* split, double* box,
+                   int32_t* child, int32_t* father, int32_t* cell, int8_t* dir, int32_t* level, int64_t* nnodes) {
+    Sim* S = buildSim(sc);
+    double total = 0;
+    for (int h = 0; h < S->ncomp; h++) total += S->dustnorm[h];
+    TreeBuild T;
+    T.box.push_back(S->grid->ext); T.child.push_back(-1); T.father.push_back(-1); T.level.push_back(0);
+    T.dir.push_back(-1); T.split.push_back(0);
+    Rng rng; rng.init(seed);
+    const bool nocrit = !(maxfrac > 0);
+    vector<double> mass;
+    size_t l = 0;
+    while (l < T.box.size()) {
+        // the nodes of one level are contiguous in creation order; their masses are independent of
+        // one another (sampler 1), so a level is sampled by several threads at once
+        size_t lend = l;
+        while (lend < T.box.size() && T.level[lend] == T.level[l]) lend++;
+        const int lev = T.level[l];
+        if (lev > minlevel && lev < maxlevel && !nocrit) {
+            mass.assign(lend - l, 0.0);
+            auto body = [&](size_t q) {
+                const Box& b = T.box[q];
+                double sum = 0;
+                if (sampler == 1) {
+                    for (int n = 0; n < Nrandom; n++) {
+                        Philox ph(seed, (uint64_t)q, 0x7EE0000u + (uint32_t)n);
+                        double x = ph.uniform(), y = ph.uniform(), z = ph.uniform();
+                        sum += dust_density(*S, b.fracpos(x, y, z));
+                    }
+                } else {
+                    for (int n = 0; n < Nrandom; n++) sum += dust_density(*S, rng.position(b));
+                }
+                mass[q - l] = sum/Nrandom*b.volume();            // TreeNodeSampleDensityCalculator.cpp:42-45
+            };
+            if (sampler == 1 && nthreads > 1) {
+                std::atomic<size_t> next{l};
+                auto worker = [&]() { size_t q; while ((q = next.fetch_add(1)) < lend) body(q); };
+                vector<std::thread> th;
+                for (int t = 1; t < nthreads; t++) th.emplace_back(worker);
+                worker();
+                for (auto& t : th) t.join();
+            } else {
+                for (size_t q = l; q < lend; q++) body(q);
+            }
+        }
+        for (size_t q = l; q < lend; q++) {                          // TreeDustGrid.cpp:166-230
+            bool need;
+            if (lev <= minlevel) need = true;
+            else if (lev < maxlevel) need = nocrit || mass[q - l]/total >= maxfrac;
+            else need = false;
+            if (need) T.split_node((int)q, type);
+        }
+        l = lend;
+    }
+    const int64_t n = (int64_t)T.box.size();
+    *nnodes = n;
+    delete S->grid; delete S;
+    if (n > max_nodes) return SKG_ERR_CAPACITY;
+    int m = 0;
+    for (int64_t q = 0; q < n; q++) {
+        const Box& b = T.box[q];
+        box[6*q] = b.xmin; box[6*q+1] = b.ymin; box[6*q+2] = b.zmin;
+        box[6*q+3] = b.xmax; box[6*q+4] = b.ymax; box[6*q+5] = b.zmax;
+        split[q] = T.split[q]; child[q] = T.child[q]; father[q] = T.father[q]; dir[q] = T.dir[q];
+        level[q] = T.level[q];
+        cell[q] = T.child[q] < 0 ? m++ : -1;
+    }
+    return 0;
+}
+
 // Runs a simulation: the stellar emission phase (MonteCarloSimulation::runstellaremission,
 // MonteCarloSimulation.cpp:241-295) for `packages` per wavelength, optionally followed by
 // `selfabs_cycles` dust self-absorption cycles (fixed cycle count, PanMonteCarloSimulation.cpp:106-242,
@@ -1450,7 +1626,8 @@ int orc_sample_density(const skg_scene* sc, int nthreads, uint64_t seed, double*
 // of the phases (as the reference's TimeLogger times a phase), without the set-up.
 // cubes[i]/seds[i] receive instrument i's tallies (layout of skg_read_instrument).
 int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t seed, int selfabs_cycles,
-                 int dust_emission_phase, int64_t max_packets, double** cubes, double** seds,
+                 int dust_emission_phase, int64_t max_packets, const int32_t* ells, int nell,
+                 double** cubes, double** seds,
                  double* labs_stel, double* labs_dust, double* temperature, orc_stats* st) {
     Sim* S = buildSim(sc);
     Sim& R = *S;
@@ -1458,6 +1635,11 @@ int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t se
     if (sc->rho) R.rho.assign(sc->rho, sc->rho + nc*R.ncomp);
     else if (R.ncomp) sampleDensity(R, sc->density_samples > 0 ? sc->density_samples : 100, nthreads, seed + 1000003);
     int nl = R.nlambda;
+    // the stellar phase's wavelengths: all, or the given subset (a partial run of the same
+    // simulation: each packet still carries L_ell/Npp)
+    vector<int> ellv;
+    if (ells && nell > 0) ellv.assign(ells, ells + nell); else for (int e = 0; e < nl; e++) ellv.push_back(e);
+    const int nsel = (int)ellv.size();
     uint64_t Nchunks, chunksize, Npp;
     chunkParams(packages, nthreads, 1, nl, Nchunks, chunksize, Npp);
     std::atomic<int64_t> launched{0};
@@ -1465,8 +1647,8 @@ int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t se
     const auto t_loop = std::chrono::steady_clock::now();
 
     // stellar emission (MonteCarloSimulation.cpp:259-295)
-    parallelCall(nthreads, (uint64_t)nl*Nchunks, seed, [&](uint64_t index, Rng& rng) {
-        int ell = index % nl;
+    parallelCall(nthreads, (uint64_t)nsel*Nchunks, seed, [&](uint64_t index, Rng& rng) {
+        int ell = ellv[index % nsel];
         double L = R.Lv[ell]/Npp;
         if (!(L > 0)) return;
         double Lthreshold = L/R.minWeightReduction;

@@ -67,7 +67,7 @@ def lib():
         if not os.path.exists(LIB):
             build()
         L = C.CDLL(LIB)
-        L.orc_trace_paths.argtypes = [C.c_void_p, dp, dp, C.c_int64, i32p, dp, i64p, C.c_int64, i64p]
+        L.orc_trace_paths.argtypes = [C.c_void_p, dp, dp, C.c_int64, i32p, dp, i64p, C.c_int64, i64p, C.c_int]
         L.orc_optical_depth.argtypes = [C.c_void_p, dp, dp, C.c_int64, C.c_int, dp]
         L.orc_pathlength.restype = C.c_double
         L.orc_pathlength.argtypes = [dp, dp, C.c_int, C.c_double]
@@ -80,13 +80,20 @@ def lib():
         L.orc_sample_density.argtypes = [C.c_void_p, C.c_int, C.c_uint64, dp]
         L.orc_chunk_params.argtypes = [C.c_double, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint64),
                                        C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
-        L.orc_simulate.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_int64,
+        L.orc_tree_build.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_uint64, C.c_int,
+                                     C.c_int, C.c_int64, C.POINTER(C.c_uint8), dp, i32p, i32p, i32p,
+                                     C.POINTER(C.c_int8), i32p, i64p]
+        L.orc_simulate.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_int64, i32p,
+                                   C.c_int,
                                    C.POINTER(dp), C.POINTER(dp), dp, dp, dp, C.POINTER(Stats)]
         _lib = L
     return _lib
 
 
-def trace_paths(model, r, k):
+def trace_paths(model, r, k, nthreads=None):
+    """DustGrid::path for every ray: (offsets, cells, ds), segments of ray i at
+    offsets[i]..offsets[i+1]-1; traced by nthreads threads (default: all cores)."""
+    nthreads = nthreads or os.cpu_count() or 1
     sc, keep = model.lower()
     r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
     k = np.ascontiguousarray(k, dtype=np.float64).reshape(-1, 3)
@@ -98,14 +105,14 @@ def trace_paths(model, r, k):
     ds = np.zeros(1)
     L = lib()
     rc = L.orc_trace_paths(C.byref(sc), r.ctypes.data_as(dp), k.ctypes.data_as(dp), n, cells.ctypes.data_as(i32p),
-                           ds.ctypes.data_as(dp), off.ctypes.data_as(i64p), cap, fb.ctypes.data_as(i64p))
+                           ds.ctypes.data_as(dp), off.ctypes.data_as(i64p), cap, fb.ctypes.data_as(i64p), nthreads)
     if rc == 8:
         cap = int(off[n])
         cells = np.zeros(max(cap, 1), dtype=np.int32)
         ds = np.zeros(max(cap, 1))
         rc = L.orc_trace_paths(C.byref(sc), r.ctypes.data_as(dp), k.ctypes.data_as(dp), n,
                                cells.ctypes.data_as(i32p), ds.ctypes.data_as(dp), off.ctypes.data_as(i64p), cap,
-                               fb.ctypes.data_as(i64p))
+                               fb.ctypes.data_as(i64p), nthreads)
     assert rc == 0
     tot = int(off[n])
     return off, cells[:tot], ds[:tot]
@@ -128,8 +135,10 @@ def sample_density(model, nthreads=8, seed=99):
     return rho.reshape(len(model.dustComps), -1)
 
 
-def simulate(model, packages, nthreads=8, seed=4357, selfabs_cycles=0, dust_emission_phase=False, max_packets=0):
-    """Runs the restated life cycle; returns dict(cubes, seds, labs_stel, labs_dust, T, stats)."""
+def simulate(model, packages, nthreads=8, seed=4357, selfabs_cycles=0, dust_emission_phase=False, max_packets=0,
+             ells=None):
+    """Runs the restated life cycle; returns dict(cubes, seds, labs_stel, labs_dust, T, stats).
+    ells: run the stellar phase for these wavelength indices only (default: all)."""
     sc, keep = model.lower()
     nl = model.wavelengthGrid.Nlambda
     ncomp = []
@@ -155,9 +164,71 @@ def simulate(model, packages, nthreads=8, seed=4357, selfabs_cycles=0, dust_emis
     ld = np.zeros(ncells * nl)
     T = np.zeros(max(ncells, 1))
     st = Stats()
+    ev = np.ascontiguousarray(ells if ells is not None else [], dtype=np.int32)
     assert lib().orc_simulate(C.byref(sc), float(packages), nthreads, seed, selfabs_cycles, int(dust_emission_phase),
-                              int(max_packets), cp, sp, ls.ctypes.data_as(dp), ld.ctypes.data_as(dp),
+                              int(max_packets), ev.ctypes.data_as(i32p) if len(ev) else None, len(ev), cp, sp, ls.ctypes.data_as(dp), ld.ctypes.data_as(dp),
                               T.ctypes.data_as(dp), C.byref(st)) == 0
     stats = {n: getattr(st, n) for n, _ in Stats._fields_}
     return dict(cubes=cubes, seds=seds, labs_stel=ls.reshape(ncells, nl), labs_dust=ld.reshape(ncells, nl),
                 T=T[:ncells], stats=stats)
+
+
+def tree_build(model, gtype, extent, minLevel=2, maxLevel=6, maxMassFraction=1e-6, samples=100, seed=4357,
+               sampler=0, nthreads=8, neighbors=True):
+    """TreeDustGrid construction restated on the CPU (oracle.cpp: orc_tree_build, following
+    TreeDustGrid.cpp:80-230).  sampler 0 draws node samples from the reference's MT19937
+    (Random::position); sampler 1 from the counter-based streams of the library's device builder.
+    With neighbors=True the neighbour lists come from the reference's own node classes compiled
+    in oracle/_ref (ref_tree_neighbors, OctTreeNode/BinTreeNode::addneighbors + sortneighbors),
+    given the split decisions.  Returns (TreeDustGrid, split flags, levels)."""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, ".."))
+    from skirt7_b200.scene import CartesianDustGrid, TreeDustGrid
+    from skirt7_b200 import _abi as A
+    model.normalise()
+    saved = model.dustGrid
+    x0, y0, z0, x1, y1, z1 = extent
+    model.dustGrid = CartesianDustGrid(x0, x1, y0, y1, z0, z1, 1, 1, 1)   # only the extent is read
+    sc, keep = model.lower()
+    model.dustGrid = saved
+    L = lib()
+    nn = C.c_int64(0)
+    cap = 1
+    while True:
+        split = np.zeros(cap, dtype=np.uint8)
+        box = np.zeros(6 * cap)
+        child, father, cell, lev = (np.zeros(cap, dtype=np.int32) for _ in range(4))
+        d = np.zeros(cap, dtype=np.int8)
+        rc = L.orc_tree_build(C.byref(sc), gtype, minLevel, maxLevel, maxMassFraction, samples, seed, sampler, nthreads,
+                              cap, split.ctypes.data_as(C.POINTER(C.c_uint8)), box.ctypes.data_as(dp),
+                              child.ctypes.data_as(i32p), father.ctypes.data_as(i32p), cell.ctypes.data_as(i32p),
+                              d.ctypes.data_as(C.POINTER(C.c_int8)), lev.ctypes.data_as(i32p), C.byref(nn))
+        if rc == 0:
+            break
+        assert rc == 8, rc
+        cap = nn.value
+    n = nn.value
+    off = np.zeros(6 * n + 1, dtype=np.int64)
+    ids = np.zeros(1, dtype=np.int32)
+    search = A.SEARCH_TOPDOWN
+    if neighbors:
+        R = ref()
+        if R is None:
+            raise RuntimeError("neighbour lists need the reference's node classes (oracle/_ref)")
+        t = 1 if gtype == A.GRID_OCTREE else 2
+        ex = np.array(extent, dtype=np.float64)
+        rbox = np.zeros(6 * n)
+        maxids = 16 * n
+        while True:
+            ids = np.zeros(maxids, dtype=np.int32)
+            q = R.ref_tree_neighbors(t, ex.ctypes.data_as(dp), split.ctypes.data_as(C.POINTER(C.c_uint8)), n, n,
+                                     rbox.ctypes.data_as(dp), off.ctypes.data_as(i64p), ids.ctypes.data_as(i32p),
+                                     maxids)
+            if q >= 0:
+                break
+            maxids = -q
+        assert q == n and np.array_equal(rbox, box[: 6 * n]), "reference node boxes differ from the restated ones"
+        ids = ids[: off[-1]]
+        search = A.SEARCH_NEIGHBOR
+    grid = TreeDustGrid(gtype, tuple(extent), box[: 6 * n], child[:n], father[:n], cell[:n], d[:n], off, ids, search)
+    return grid, split[:n], lev[:n]

@@ -337,7 +337,14 @@ struct skg_ctx {
     int64_t ncells = 0;
     std::vector<int64_t> cube_len, sed_len;
     unsigned long long* counters = nullptr;   // = own.counters
-    unsigned* err = nullptr;                  // = own.err
+    unsigned* err = nullptr;                  // = own.err (the phases' error word)
+    // The path harness (skg_trace_paths, skg_optical_depth, skg_trace_paths_noalloc) flags its
+    // errors in a word of its own, so that a harness call never clears a finished phase's flags
+    // before skg_sync has reported them.  hev marks the end of the last no-alloc call on the
+    // caller's stream; skg_sync waits for it before it reads herr.
+    unsigned* herr = nullptr;
+    cudaEvent_t hev = nullptr;
+    bool hev_pending = false;
     Staging own;                              // tables of this context's own launches
     WaveRunner waves;                         // packet pool and job lists of this context's phases
     uint64_t wave_count = 0;                  // waves since the last tally reset
@@ -608,6 +615,10 @@ int skg_ctx_create(const skg_scene* sc, int device, skg_ctx** out) {
         CK(cudaMemsetAsync(ctx->own.err, 0, sizeof(unsigned), s));
         ctx->counters = ctx->own.counters;
         ctx->err = ctx->own.err;
+        ctx->herr = A.alloc<unsigned>(1);
+        if (!ctx->herr) throw Failure{SKG_ERR_OOM, "device allocation failed"};
+        CK(cudaMemsetAsync(ctx->herr, 0, sizeof(unsigned), s));
+        CK(cudaEventCreateWithFlags(&ctx->hev, cudaEventDisableTiming));
         ctx->ds = upload(A, &H, 1, s);
         CK(cudaStreamSynchronize(s));
         *out = ctx;
@@ -619,6 +630,7 @@ int skg_ctx_create(const skg_scene* sc, int device, skg_ctx** out) {
         ctx->A.release();
         if (ctx->ev0) cudaEventDestroy(ctx->ev0);
         if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+        if (ctx->hev) cudaEventDestroy(ctx->hev);
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
         delete ctx;
         return rc;
@@ -629,8 +641,9 @@ int skg_ctx_destroy(skg_ctx* ctx) {
     if (!ctx) return SKG_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->hev_pending) cudaEventSynchronize(ctx->hev);
     ctx->A.release();
-    cudaEventDestroy(ctx->ev0); cudaEventDestroy(ctx->ev1);
+    cudaEventDestroy(ctx->ev0); cudaEventDestroy(ctx->ev1); cudaEventDestroy(ctx->hev);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SKG_OK;
@@ -649,19 +662,32 @@ int skg_sync(skg_ctx* ctx, int timeout_ms) {
     if (rc) return rc;
     cudaSetDevice(ctx->device);
     auto t0 = std::chrono::steady_clock::now();
-    while (true) {
-        cudaError_t e = cudaStreamQuery(ctx->stream);
-        if (e == cudaSuccess) break;
-        if (e != cudaErrorNotReady) { cudaGetLastError(); return fail(ctx, Failure{SKG_ERR_CUDA, cudaGetErrorString(e)}); }
-        if (timeout_ms >= 0 && std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() > timeout_ms)
-            return fail(ctx, Failure{SKG_ERR_TIMEOUT, "timed out waiting for the device"});
-        std::this_thread::sleep_for(std::chrono::microseconds(200));
+    // the context stream, then the end of the last no-alloc harness call on the caller's stream
+    for (int what = 0; what < 2; what++) {
+        if (what == 1 && !ctx->hev_pending) break;
+        while (true) {
+            cudaError_t e = what == 0 ? cudaStreamQuery(ctx->stream) : cudaEventQuery(ctx->hev);
+            if (e == cudaSuccess) break;
+            if (e != cudaErrorNotReady) { cudaGetLastError(); return fail(ctx, Failure{SKG_ERR_CUDA, cudaGetErrorString(e)}); }
+            if (timeout_ms >= 0 && std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() > timeout_ms)
+                return fail(ctx, Failure{SKG_ERR_TIMEOUT, "timed out waiting for the device"});
+            std::this_thread::sleep_for(std::chrono::microseconds(200));
+        }
     }
-    unsigned err = 0;
+    ctx->hev_pending = false;
+    unsigned err = 0, herr = 0;
     cudaMemcpy(&err, ctx->err, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    cudaMemcpy(&herr, ctx->herr, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    if (herr) {
+        // a harness failure is reported once
+        cudaMemsetAsync(ctx->herr, 0, sizeof(unsigned), ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+    }
     if (err & ERR_NAN_TAU) return fail(ctx, Failure{SKG_ERR_NAN_TAU, "The optical depth along the path is not a positive number"});
     if (err & (ERR_STEP_BUDGET | ERR_SCATT_BUDGET)) return fail(ctx, Failure{SKG_ERR_STEP_BUDGET, "a packet exceeded its step or scattering budget"});
-    if (err & ERR_CAPACITY) return fail(ctx, Failure{SKG_ERR_CAPACITY, "segment buffer too small"});
+    if (err & ERR_CAPACITY) return fail(ctx, Failure{SKG_ERR_CAPACITY, "a packet pool or job list overflowed"});
+    if (herr & ERR_CAPACITY) return fail(ctx, Failure{SKG_ERR_CAPACITY, "segment buffer too small"});
+    if (herr & ERR_STEP_BUDGET) return fail(ctx, Failure{SKG_ERR_STEP_BUDGET, "a path exceeded the step budget"});
     return SKG_OK;
 }
 
@@ -679,6 +705,10 @@ int skg_read_density(skg_ctx* ctx, double* rho) {
 int skg_trace_paths(skg_ctx* ctx, const double* r, const double* k, int64_t n, int precision,
                     int32_t* cells, double* ds, int64_t* offsets, int64_t capacity) {
     if (!ctx || n < 0 || !offsets) return SKG_ERR_INVALID;
+    if (precision != SKG_PREC_FP32 && precision != SKG_PREC_FP64)
+        return fail(ctx, Failure{SKG_ERR_INVALID, "skg_trace_paths: unknown precision"});
+    int rc = settle(ctx, -1);
+    if (rc) return rc;
     try {
         CK(cudaSetDevice(ctx->device));
         cudaStream_t s = ctx->stream;
@@ -687,8 +717,8 @@ int skg_trace_paths(skg_ctx* ctx, const double* r, const double* k, int64_t n, i
         double* dk = upload(T, k, 3 * (size_t)n, s);
         int64_t* cnt = T.alloc<int64_t>(n + 1);
         if (!cnt) throw Failure{SKG_ERR_OOM, "device allocation failed"};
-        CK(cudaMemsetAsync(ctx->err, 0, sizeof(unsigned), s));
-        CK(launch_count_segments(ctx->grid, dr, dk, n, precision, cnt, ctx->err, s));
+        CK(cudaMemsetAsync(ctx->herr, 0, sizeof(unsigned), s));
+        CK(launch_count_segments(ctx->grid, dr, dk, n, precision, cnt, ctx->herr, s));
         std::vector<int64_t> hc(n);
         if (n) CK(cudaMemcpyAsync(hc.data(), cnt, n * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
@@ -700,14 +730,15 @@ int skg_trace_paths(skg_ctx* ctx, const double* r, const double* k, int64_t n, i
         int32_t* dc = T.alloc<int32_t>(tot);
         double* dd = T.alloc<double>(tot);
         if (!dc || !dd) throw Failure{SKG_ERR_OOM, "device allocation failed"};
-        CK(launch_write_segments(ctx->grid, dr, dk, n, precision, doff, dc, dd, ctx->err, s));
+        CK(launch_write_segments(ctx->grid, dr, dk, n, precision, doff, dc, dd, ctx->herr, s));
         if (tot) {
             CK(cudaMemcpyAsync(cells, dc, tot * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
             CK(cudaMemcpyAsync(ds, dd, tot * sizeof(double), cudaMemcpyDeviceToHost, s));
         }
-        CK(cudaStreamSynchronize(s));
         unsigned err = 0;
-        CK(cudaMemcpy(&err, ctx->err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(&err, ctx->herr, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemsetAsync(ctx->herr, 0, sizeof(unsigned), s));    // reported here, not again by skg_sync
+        CK(cudaStreamSynchronize(s));
         if (err & ERR_STEP_BUDGET) throw Failure{SKG_ERR_STEP_BUDGET, "a path exceeded the step budget"};
         if (err & ERR_CAPACITY) throw Failure{SKG_ERR_CAPACITY, "segment count changed between passes"};
         return SKG_OK;
@@ -716,6 +747,10 @@ int skg_trace_paths(skg_ctx* ctx, const double* r, const double* k, int64_t n, i
 
 int skg_optical_depth(skg_ctx* ctx, const double* r, const double* k, int64_t n, int ell, int precision, double* tau) {
     if (!ctx || n < 0 || ell < 0 || ell >= ctx->nlambda) return SKG_ERR_INVALID;
+    if (precision != SKG_PREC_FP32 && precision != SKG_PREC_FP64)
+        return fail(ctx, Failure{SKG_ERR_INVALID, "skg_optical_depth: unknown precision"});
+    int rc = settle(ctx, -1);
+    if (rc) return rc;
     try {
         CK(cudaSetDevice(ctx->device));
         cudaStream_t s = ctx->stream;
@@ -723,10 +758,15 @@ int skg_optical_depth(skg_ctx* ctx, const double* r, const double* k, int64_t n,
         double* dr = upload(T, r, 3 * (size_t)n, s);
         double* dk = upload(T, k, 3 * (size_t)n, s);
         double* dt = T.alloc<double>(n);
-        CK(cudaMemsetAsync(ctx->err, 0, sizeof(unsigned), s));
-        CK(launch_optical_depth(ctx->grid, ctx->ds, dr, dk, n, ell, precision, dt, ctx->err, s));
+        if (n && !dt) throw Failure{SKG_ERR_OOM, "device allocation failed"};
+        CK(cudaMemsetAsync(ctx->herr, 0, sizeof(unsigned), s));
+        CK(launch_optical_depth(ctx->grid, ctx->ds, dr, dk, n, ell, precision, dt, ctx->herr, s));
         if (n) CK(cudaMemcpyAsync(tau, dt, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        unsigned err = 0;
+        CK(cudaMemcpyAsync(&err, ctx->herr, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemsetAsync(ctx->herr, 0, sizeof(unsigned), s));
         CK(cudaStreamSynchronize(s));
+        if (err & ERR_STEP_BUDGET) throw Failure{SKG_ERR_STEP_BUDGET, "a path exceeded the step budget"};
         return SKG_OK;
     } catch (const Failure& f) { return fail(ctx, f); }
 }
@@ -744,6 +784,7 @@ int skg_run_phase(skg_ctx* ctx, int phase, const int32_t* ells, int nell, uint64
         REQUIRE(count <= npp || npp == 0, "packet range exceeds the packet count");
         if (phase != SKG_PHASE_STELLAR) REQUIRE(ctx->emit_cdf != nullptr, "dust phases need dust emission enabled");
         REQUIRE(!opts || opts->pool >= 0, "negative packet pool");
+        REQUIRE(!opts || opts->precision == SKG_PREC_FP32 || opts->precision == SKG_PREC_FP64, "unknown precision");
         cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
         if (count == 0) return SKG_OK;
         const uint64_t total = (uint64_t)nell * count;
@@ -1205,6 +1246,7 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
         int precision = opts ? opts->precision : SKG_PREC_FP32;
         int blocks = opts ? opts->blocks : 0;
         REQUIRE(!opts || opts->pool >= 0, "negative packet pool");
+        REQUIRE(!opts || opts->precision == SKG_PREC_FP32 || opts->precision == SKG_PREC_FP64, "unknown precision");
         // the pool: enough records for the batch up to the pool limit, rounded up to a power of two
         // so that replays of a captured graph keep fitting
         const size_t pool_max = (opts && opts->pool > 0) ? (size_t)opts->pool : ((size_t)1 << 21);
@@ -1388,6 +1430,12 @@ int skg_trace_paths_noalloc(skg_ctx* ctx, const double* d_r, const double* d_k, 
                                  " rays exceed the per-call maximum of " + std::to_string(NA_MAX_RAYS)});
     if (!ctx || n < 0 || capacity < 0 || !d_offsets || (n > 0 && (!d_r || !d_k)) || (capacity > 0 && (!d_cells || !d_ds)))
         return fail(ctx, Failure{SKG_ERR_INVALID, "skg_trace_paths_noalloc: invalid arguments"});
+    if (precision != SKG_PREC_FP32 && precision != SKG_PREC_FP64)
+        return fail(ctx, Failure{SKG_ERR_INVALID, "skg_trace_paths_noalloc: unknown precision"});
+    // a phase still running on the context finishes first (its waves complete; its error flags
+    // stay in the phase word for skg_sync)
+    int rc = settle(ctx, -1);
+    if (rc) return rc;
     try {
         CK(cudaSetDevice(ctx->device));
         REQUIRE(ctx->device >= 0 && ctx->device < 64, "device ordinal out of range");
@@ -1404,20 +1452,23 @@ int skg_trace_paths_noalloc(skg_ctx* ctx, const double* d_r, const double* d_k, 
         }
         int64_t* block_tot = scratch + NA_MAX_RAYS + 1;
         cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-        CK(cudaMemsetAsync(ctx->err, 0, sizeof(unsigned), s));
+        CK(cudaMemsetAsync(ctx->herr, 0, sizeof(unsigned), s));
         if (n == 0) {
             CK(cudaMemsetAsync(d_offsets, 0, sizeof(int64_t), s));
-            return SKG_OK;
+        } else {
+            int nblocks = (int)((n + NA_SCAN - 1) / NA_SCAN);
+            CK(launch_count_segments(ctx->grid, d_r, d_k, n, precision, scratch, ctx->herr, s));
+            na_scan_blocks<<<nblocks, NA_SCAN, 0, s>>>(scratch, n, d_offsets, block_tot);
+            CK(cudaGetLastError());
+            na_scan_totals<<<1, NA_SCAN, 0, s>>>(block_tot, nblocks, capacity, ctx->herr);
+            CK(cudaGetLastError());
+            na_add_offsets<<<nblocks, NA_SCAN, 0, s>>>(d_offsets, block_tot, n, capacity, scratch);
+            CK(cudaGetLastError());
+            CK(launch_write_segments(ctx->grid, d_r, d_k, n, precision, scratch, d_cells, d_ds, ctx->herr, s));
         }
-        int nblocks = (int)((n + NA_SCAN - 1) / NA_SCAN);
-        CK(launch_count_segments(ctx->grid, d_r, d_k, n, precision, scratch, ctx->err, s));
-        na_scan_blocks<<<nblocks, NA_SCAN, 0, s>>>(scratch, n, d_offsets, block_tot);
-        CK(cudaGetLastError());
-        na_scan_totals<<<1, NA_SCAN, 0, s>>>(block_tot, nblocks, capacity, ctx->err);
-        CK(cudaGetLastError());
-        na_add_offsets<<<nblocks, NA_SCAN, 0, s>>>(d_offsets, block_tot, n, capacity, scratch);
-        CK(cudaGetLastError());
-        CK(launch_write_segments(ctx->grid, d_r, d_k, n, precision, scratch, d_cells, d_ds, ctx->err, s));
+        // skg_sync waits for this point of the caller's stream before it reads the harness flags
+        CK(cudaEventRecord(ctx->hev, s));
+        ctx->hev_pending = true;
         return SKG_OK;
     } catch (const Failure& f) { return fail(ctx, f); }
 }

@@ -1,6 +1,7 @@
 """skg_trace_paths_noalloc (device buffers in and out, scratch in a static device array) gives
-the same offsets, cells and segment lengths as skg_trace_paths, call after call, and allocates
-no device memory.  Named so that it is collected after every other test file."""
+the same offsets, cells and segment lengths as skg_trace_paths, call after call (up to the
+largest call the scratch array holds), allocates no device memory, and leaves the error flags of
+a finished phase for skg_sync.  Named so that it is collected after every other test file."""
 import numpy as np
 import pytest
 
@@ -17,8 +18,8 @@ torch = pytest.importorskip("torch")
 EXT = (-20 * KPC, -20 * KPC, -2 * KPC, 20 * KPC, 20 * KPC, 2 * KPC)
 
 
-def _ctx():
-    m = models.oligo_disk(N=(100, 100, 50))
+def _ctx(N=(100, 100, 50)):
+    m = models.oligo_disk(N=N)
     m.rho = cell_center_density(m)
     return runtime.Context(m)
 
@@ -79,4 +80,49 @@ def test_noalloc_limits():
     o, _, _, _ = _noalloc(ctx, r[:0], k[:0], 0, A.PREC_FP64, stream)
     assert o.tolist() == [0]
     ctx.sync()
+    ctx.close()
+
+
+def test_noalloc_at_the_maximum_ray_count():
+    """n = SKG_NOALLOC_MAX_RAYS: the scan of the block totals runs at its full width (1024
+    blocks of 1024 rays); the offsets, cells and lengths equal skg_trace_paths' on a small grid."""
+    ctx = _ctx(N=(16, 16, 8))
+    stream = torch.cuda.Stream()
+    n = runtime.Context.NOALLOC_MAX_RAYS
+    r, k = seeded_rays(n, EXT, seed=51, disk=(4 * KPC, 0.35 * KPC))
+    o_ref, c_ref, d_ref = ctx.trace_paths(r, k, A.PREC_FP64)
+    tot = int(o_ref[-1])
+    o, c, d, _ = _noalloc(ctx, r, k, tot, A.PREC_FP64, stream)
+    ctx.sync()
+    assert np.array_equal(o, o_ref)
+    assert np.array_equal(c[:tot], c_ref) and np.array_equal(d[:tot], d_ref)
+    ctx.close()
+
+
+def test_noalloc_keeps_the_phase_flags():
+    """A phase whose packets ran out of their step budget (max_steps = 1) flags the context; a
+    no-alloc path call made afterwards finishes that phase first and keeps its flag, so skg_sync
+    still reports the phase's failure; the path call itself succeeds and its results are right."""
+    ctx = _ctx(N=(20, 20, 10))
+    stream = torch.cuda.Stream()
+    ctx.run_phase(A.PHASE_STELLAR, [0], 20000, 0, 20000, seed=5, max_steps=1)
+    r, k = seeded_rays(3000, EXT, seed=61)
+    o_ref, c_ref, d_ref = ctx.trace_paths(r, k, A.PREC_FP64)
+    tot = int(o_ref[-1])
+    o, c, d, _ = _noalloc(ctx, r, k, tot, A.PREC_FP64, stream)
+    with pytest.raises(A.SkirtError) as e:
+        ctx.sync()
+    assert e.value.code == A.SKG_ERR_STEP_BUDGET
+    assert np.array_equal(o, o_ref) and np.array_equal(c[:tot], c_ref) and np.array_equal(d[:tot], d_ref)
+    # an unknown precision is rejected before any work is enqueued (real buffers, so that only
+    # the precision is wrong)
+    dr = torch.from_numpy(np.ascontiguousarray(r[:10])).cuda()
+    dk = torch.from_numpy(np.ascontiguousarray(k[:10])).cuda()
+    cells = torch.zeros(4096, dtype=torch.int32, device="cuda")
+    ds = torch.zeros(4096, dtype=torch.float64, device="cuda")
+    off = torch.zeros(11, dtype=torch.int64, device="cuda")
+    with pytest.raises(A.SkirtError) as e:
+        ctx.trace_paths_noalloc(dr.data_ptr(), dk.data_ptr(), 10, cells.data_ptr(), ds.data_ptr(), off.data_ptr(),
+                                4096, 7, None)
+    assert e.value.code == A.SKG_ERR_INVALID and "precision" in str(e.value)
     ctx.close()
