@@ -11,14 +11,20 @@ other configurations of the hot path with the same machinery:
                     dust-emission phase
 
 One step = the workload's phases (a sequence of waves: an event pass and a traversal pass each)
-over all wavelengths with --packets packets per wavelength per GPU.  Ranks (torchrun, one per GPU)
-run disjoint packet ranges of one simulation and all-reduce the frames over NCCL at the end of
-each step (weak scaling: the packets per GPU are fixed).  `value` is device-timed; `e2e` is the
-same metric through the C ABI with the tallies read back into host memory every step.
+over all wavelengths with --packets packets per wavelength per GPU (10^7 by default, the
+configuration's count).  A step ends when its phases have finished (the host has seen the last
+wave's counters), so every step times exactly its own waves.  Ranks (one process per GPU; with
+--gpus N and no torchrun environment the script starts the N ranks itself) run disjoint packet
+ranges of one simulation and all-reduce the frames over NCCL at the end of each step (weak
+scaling: the packets per GPU are fixed).  `value` is device-timed; `e2e` is the same metric
+through the C ABI with the tallies read back into host memory every step.
 
 --impl reference times the reference's algorithm on the host cores: the oracle (a scalar FP64
 restatement of the reference's life cycle, oracle/oracle.cpp) with all host threads on a
-bounded sample of the same workload.
+bounded sample of the same workload.  Its inputs are built on the host alone -- the tree by the
+oracle's restated subdivision with the reference's node classes (oracle/_ref), the Voronoi grid
+by Voro++, the cell densities by the oracle's DustSystem sampling -- so that arm loads none of
+this repository's device code.
 """
 import argparse
 import json
@@ -43,7 +49,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="octree_pan", choices=WORKLOADS)
-    p.add_argument("--packets", type=float, default=1e6, help="packets per wavelength per GPU per step")
+    p.add_argument("--packets", type=float, default=1e7, help="packets per wavelength per GPU per step")
+    p.add_argument("--e2e-steps", type=int, default=5, help="steps of the end-to-end leg (at most --steps)")
     p.add_argument("--max-level", type=int, default=10)
     p.add_argument("--mass-fraction", type=float, default=1e-6)
     p.add_argument("--nlambda", type=int, default=50)
@@ -109,22 +116,28 @@ class Clocks:
 # ---------------------------------------------------------------------------------------------
 # workloads
 
-class Workload:
-    """A configuration: its scene (grid built on the device), the phases of one step and the
-    algorithmic bytes of its traversal pass."""
+KDTREE_MASS_FRACTION = 3e-7     # the k-d tree workload's cell mass fraction: ~4.2*10^6 leaves
 
-    def __init__(self, args, device):
+
+class Workload:
+    """A configuration: its scene, the phases of one step and the algorithmic bytes of its
+    traversal pass.  host=True builds the grid on the host alone (the reference arm: the oracle's
+    restated tree subdivision with the device builder's node sampler, so the tree is the same;
+    Voro++ for the Voronoi grid); otherwise on the device."""
+
+    def __init__(self, args, device, host=False):
         from skirt7_b200 import _abi as A
-        from skirt7_b200 import models, runtime
+        from skirt7_b200 import models
         from skirt7_b200.scene import KPC
         self.name = args.workload
         self.grid_s = 0.0
         self.dust_phase = False
+        self.selfabs_cycles = 0
         ext = (-20 * KPC, -20 * KPC, -2 * KPC, 20 * KPC, 20 * KPC, 2 * KPC)
         t0 = time.time()
         if self.name == "octree_pan":
             self.model = models.pan_disk(nlambda=args.nlambda, inclinations=(0, 60, 88), npix=512)
-            self.model.dustGrid, self.grid_s = get_tree(args, self.model, device)
+            self.model.dustGrid, self.grid_s = get_tree(args, self.model, device, host)
             self.metric = "photon packets/s (stellar emission, octree pan disk)"
             self.desc = ("panchromatic octree disk galaxy: %d wavelengths 0.1-10 micron, octree max level %d, mass "
                          "fraction %g (%d leaves), 3 frames 512x512 at 0/60/88 deg" %
@@ -146,7 +159,11 @@ class Workload:
                 q = models.sample_expdisk(base, n, rng).reshape(-1, 3)
                 d = np.concatenate([d, q[np.all((q > lo) & (q < hi), axis=1)]])
             sites = np.concatenate([d[: int(0.8 * n)], lo + rng.random((n - int(0.8 * n), 3)) * (hi - lo)])
-            self.model.dustGrid = runtime.build_voronoi(sites, ext, device)
+            if host:
+                self.model.dustGrid = _oracle().voronoi_mesh(sites, ext)
+            else:
+                from skirt7_b200 import runtime
+                self.model.dustGrid = runtime.build_voronoi(sites, ext, device)
             self.grid_s = time.time() - t0
             self.metric = "photon packets/s (clumpy disk, Voronoi grid)"
             self.desc = ("clumpy dust disk at 0.55 micron (tau_V 5, 10^4 cubic-spline clumps with 25 %% of the "
@@ -155,16 +172,23 @@ class Workload:
         else:
             self.model = models.pan_disk(nlambda=100, lmin=0.1e-6, lmax=1000e-6, inclinations=(60,), npix=512,
                                          point_fraction=0.1, dust_emission=True, write_absorption=True)
-            self.model.dustGrid = runtime.build_tree(self.model, A.GRID_BINTREE, ext, minLevel=6, maxLevel=30,
-                                                     maxMassFraction=args.mass_fraction / 2, sampleCount=100,
-                                                     seed=4357, device=device)
+            if host:
+                self.model.dustGrid, _, _ = _oracle().tree_build(self.model, A.GRID_BINTREE, ext, 6, 30,
+                                                                 KDTREE_MASS_FRACTION, 100, 4357, sampler=1,
+                                                                 nthreads=os.cpu_count() or 1)
+            else:
+                from skirt7_b200 import runtime
+                self.model.dustGrid = runtime.build_tree(self.model, A.GRID_BINTREE, ext, minLevel=6, maxLevel=30,
+                                                         maxMassFraction=KDTREE_MASS_FRACTION, sampleCount=100,
+                                                         seed=4357, device=device)
             self.grid_s = time.time() - t0
             self.dust_phase = True
-            self.metric = "photon packets/s (stellar + dust emission, k-d tree pan disk)"
+            self.selfabs_cycles = 2
+            self.metric = "photon packets/s (stellar + dust self-absorption + dust emission, k-d tree pan disk)"
             self.desc = ("panchromatic disk + point source (10 %% of L) with grey-body dust emission: k-d tree "
                          "(alternating, %d leaves), 100 wavelengths 0.1-1000 micron, 512x512 frame at 60 deg; "
-                         "a step is the stellar phase, the dust emission spectra and the dust-emission phase"
-                         % self.model.dustGrid.ncells)
+                         "a step is the stellar phase, 2 dust self-absorption cycles and the dust-emission phase "
+                         "(dust emission spectra recomputed before each dust phase)" % self.model.dustGrid.ncells)
         self.model.rho = None
         self.gtype = type(self.model.dustGrid).__name__
 
@@ -183,23 +207,29 @@ class Workload:
             b = c["steps"] * 28 * f + c["nbr_scanned"] * 4
         return b + 8 * c["absorb_adds"]
 
-    # DRAM bytes per cell step of the traversal pass, measured with ncu
-    # (dram__bytes_read.sum + dram__bytes_write.sum summed over every traversal launch of one
-    # stellar phase, divided by the phase's cell steps; profiles/traffic_per_step.md), FP32 walk
-    NCU_DRAM_BYTES_PER_STEP = {"octree_pan": 11.40, "cartesian_oligo": 3.37, "voronoi_clumpy": 260.6,
-                               "kdtree_dust": 47.9}
+    # DRAM bytes per cell step of the headline traversal pass (FP32 walk), from one ncu capture
+    # (dram__bytes_read.sum + dram__bytes_write.sum over the traversal launches of a stellar phase
+    # of this workload, divided by that phase's cell steps); roofline.traffic scales it by a
+    # launch's cell steps, and says so.  Other workloads report no traffic.
+    NCU_DRAM_BYTES_PER_STEP = {"octree_pan": 11.40}
 
     def frames(self):
         from skirt7_b200 import _abi as A
         return [i for i, ins in enumerate(self.model.instruments) if ins.type != A.INSTR_SED]
 
 
-def get_tree(args, model, device):
-    """The octree of the headline workload (device-sampled subdivision); cached across runs of the
-    same size."""
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    return oracle
+
+
+def get_tree(args, model, device, host=False):
+    """The octree of the headline workload: built on the device (device-sampled subdivision), or
+    on the host by the oracle's restated subdivision with the same node sampler (the same tree);
+    cached across runs of the same size."""
     import numpy as np
     from skirt7_b200 import _abi as A
-    from skirt7_b200 import runtime
     from skirt7_b200.scene import KPC, TreeDustGrid
     ext = (-20 * KPC, -20 * KPC, -2 * KPC, 20 * KPC, 20 * KPC, 2 * KPC)
     key = "L%d_f%g" % (args.max_level, args.mass_fraction)
@@ -209,8 +239,13 @@ def get_tree(args, model, device):
             return TreeDustGrid(A.GRID_OCTREE, ext, z["box"], z["child"], z["father"], z["cell"], z["dir"],
                                 z["off"], z["ids"]), 0.0
     t0 = time.time()
-    tree = runtime.build_tree(model, A.GRID_OCTREE, ext, minLevel=2, maxLevel=args.max_level,
-                              maxMassFraction=args.mass_fraction, sampleCount=100, seed=4357, device=device)
+    if host:
+        tree, _, _ = _oracle().tree_build(model, A.GRID_OCTREE, ext, 2, args.max_level, args.mass_fraction, 100, 4357,
+                                          sampler=1, nthreads=os.cpu_count() or 1)
+    else:
+        from skirt7_b200 import runtime
+        tree = runtime.build_tree(model, A.GRID_OCTREE, ext, minLevel=2, maxLevel=args.max_level,
+                                  maxMassFraction=args.mass_fraction, sampleCount=100, seed=4357, device=device)
     dt = time.time() - t0
     try:
         os.makedirs(os.path.dirname(args.tree_cache), exist_ok=True)
@@ -225,20 +260,18 @@ def get_tree(args, model, device):
 # the reference arm
 
 def run_reference(args, rank, world):
-    """The reference algorithm on the host cores (rank 0 only)."""
+    """The reference algorithm on the host cores (rank 0 only); everything on the host."""
     if rank != 0:
         return
-    if not _has_gpu():
-        print(json.dumps({"impl": "reference", "unavailable": "the workload's grid is built on the device; no GPU"}))
-        return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    wl = Workload(args, 0)
-    model = wl.model
-    model.rho = _density_for(model)
-    threads = os.cpu_count() or 1
+    oracle = _oracle()
     oracle.build()
-    kw = dict(dust_emission_phase=wl.dust_phase)
+    threads = os.cpu_count() or 1
+    wl = Workload(args, 0, host=True)
+    model = wl.model
+    t0 = time.time()
+    model.rho = oracle.sample_density(model, nthreads=threads, seed=4357)   # DustSystem.cpp:145-172
+    density_s = time.time() - t0
+    kw = dict(dust_emission_phase=wl.dust_phase, selfabs_cycles=wl.selfabs_cycles)
     # calibrate the sample to about --cpu-seconds per step
     probe = oracle.simulate(model, args.packets * args.gpus, nthreads=threads, seed=1, max_packets=2000, **kw)
     rate = probe["stats"]["packets"] / max(probe["stats"]["seconds"], 1e-6)
@@ -254,35 +287,34 @@ def run_reference(args, rank, world):
             "ms_per_step": 1e3 * sample / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": _config(args, wl),
+            "setup": {"grid_build_s": wl.grid_s, "density_s": density_s, "grid": "host (oracle)"},
             "cpu_baseline": {"value": v, "unit": "packets/s", "cores": threads, "kind": "port",
-                             "sample": "%d packets of the workload (all wavelengths) per step" % sample},
-            "e2e": {"value": v, "unit": "packets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                             "sample": "%d packets of the workload (all wavelengths%s) per step" %
+                                       (sample, ", all phases" if wl.dust_phase else "")},
+            "e2e": {"value": v, "unit": "packets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "native_so_loaded": _native_libs()}
     print(json.dumps(line))
 
 
-def _has_gpu():
+def _native_libs():
+    """Shared objects of this repository mapped into the process (the reference arm must show
+    oracle/ libraries only)."""
+    libs = set()
     try:
-        from skirt7_b200 import runtime
-        return runtime.device_count() > 0
-    except Exception:
-        return False
-
-
-def _density_for(model):
-    """Cell densities sampled on the device (DustSystem::setSampleDensityBody), read back so the
-    CPU baseline uses the same ones."""
-    from skirt7_b200 import runtime
-    model.rho = None
-    ctx = runtime.Context(model, 0)
-    rho = ctx.density()
-    ctx.close()
-    return rho
+        with open("/proc/self/maps") as f:
+            for ln in f:
+                p = ln.split()[-1] if ln.strip() else ""
+                if p.endswith(".so") and p.startswith(ROOT):
+                    libs.add(os.path.relpath(p, ROOT))
+    except OSError:
+        pass
+    return sorted(libs)
 
 
 def _config(args, wl):
     return {"workload": wl.desc, "name": wl.name,
             "packets_per_wavelength_per_gpu": args.packets, "nlambda": wl.model.wavelengthGrid.Nlambda,
-            "cells": wl.model.dustGrid.ncells, "grid_build_s": wl.grid_s,
+            "cells": wl.model.dustGrid.ncells,
             "geometry_precision": args.precision, "tallies": "fp64",
             "l2": "L2 flushed between timed steps (a 256 MB write on the launching stream, outside the events)",
             "parallelism": "dp%d (packet ranges per GPU, NCCL all-reduce of frames per step)" % args.gpus}
@@ -291,8 +323,23 @@ def _config(args, wl):
 # ---------------------------------------------------------------------------------------------
 # the device arm
 
+def spawn_ranks(args):
+    """--gpus N without a torchrun environment: start the N ranks (one process per GPU) under
+    torch.distributed.run on this node and return its exit status."""
+    import socket
+    sock = socket.socket()
+    sock.bind(("127.0.0.1", 0))
+    port = sock.getsockname()[1]
+    sock.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(args.gpus),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -327,17 +374,28 @@ def main():
     sizes = [_tally_len(ctx, i) for i in fr]
     # per-rank frames handed to the all-reduce (Instrument::sumResults, Instrument.cpp:57-65)
     red = [torch.zeros(n, dtype=torch.float64, device="cuda") for n in sizes] if dist else None
-    phases = [A.PHASE_STELLAR] + ([A.PHASE_DUST_EMISSION] if wl.dust_phase else [])
+    phases = ([A.PHASE_STELLAR] + [A.PHASE_DUST_SELFABS] * wl.selfabs_cycles +
+              ([A.PHASE_DUST_EMISSION] if wl.dust_phase else []))
 
     def run_phases(seed, stream):
         ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=seed, precision=prec, stream=stream)
         if wl.dust_phase:
+            # PanMonteCarloSimulation::rundustselfabsorption / rundustemission (:106-187, :191-346):
+            # before each dust phase the emission spectra follow from the absorbed luminosity
+            for c in range(wl.selfabs_cycles):
+                ctx.calc_dust_emission()
+                ctx.reset_dust_absorption()
+                ctx.run_phase(A.PHASE_DUST_SELFABS, ells, Npp, first, npp_rank, seed=seed + 2 + c, precision=prec,
+                              stream=stream)
             ctx.calc_dust_emission()            # PanDustSystem::calculatedustemission
             ctx.run_phase(A.PHASE_DUST_EMISSION, ells, Npp, first, npp_rank, seed=seed + 1, precision=prec,
                           stream=stream)
 
     def step(seed):
         run_phases(seed, handle)
+        # the phase is finished: the host has seen its last wave's counters and enqueued every wave,
+        # so the step's end event follows all of them
+        ctx.sync()
         if dist:
             with torch.cuda.stream(tstream):
                 for i, t in zip(fr, red):
@@ -388,7 +446,7 @@ def main():
     ev_ms, trav_ms, waves = ctx.phase_times()
     c = ctx.counters()
     alg_bytes = wl.alg_bytes(c, prec == A.PREC_FP32)
-    bps = wl.NCU_DRAM_BYTES_PER_STEP.get(wl.name) if prec == A.PREC_FP32 else None
+    bps = wl.NCU_DRAM_BYTES_PER_STEP.get(wl.name) if (prec == A.PREC_FP32 and args.nlambda == 50) else None
     traffic = bps * c["steps"] / max(waves, 1) if bps else None
     peak, peak_kind = peaks()
     achieved = alg_bytes / (trav_ms / 1e3) / 1e9 if trav_ms > 0 else 0.0
@@ -402,8 +460,9 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
     t0 = time.perf_counter()
-    for s in range(args.steps):
+    for s in range(e2e_steps):
         ctx.reset_tallies()
         if dist:
             ctx.sync()
@@ -421,7 +480,7 @@ def main():
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e = packets / e2e_s
+    e2e = Npp * nl * len(phases) * e2e_steps / e2e_s
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -437,18 +496,19 @@ def main():
             "ms_per_step": total_ms / args.steps, "ms_steps": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if prec == A.PREC_FP32 else "f64", "data": "synthetic",
             "config": _config(args, wl),
+            "setup": {"grid_build_s": wl.grid_s, "grid": "device"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "traffic_basis": ("ncu DRAM bytes per cell step of this workload's traversal pass "
-                                           "(%.2f B, profiles/traffic_per_step.md) x this phase's cell steps per "
-                                           "traversal pass" % bps) if bps else None,
+                         "traffic_basis": ("scaled, not measured in this run: ncu DRAM bytes per cell step of "
+                                           "this workload's traversal pass (%.2f B, one capture of a stellar "
+                                           "phase) x this launch's cell steps" % bps) if bps else None,
                          "kernel": "trav_kernel, path and peel-off instantiations (traversal pass of the stellar phase)",
                          "launch": "one traversal pass of a wave (its path-job and peel-off-job kernels)",
                          "algorithmic_bytes_per_launch": alg_bytes / max(waves, 1),
                          "kernel_ms_per_launch": trav_ms / max(waves, 1), "launches_per_phase": waves,
                          "phase_ms": kms, "event_pass_ms": ev_ms, "traversal_pass_ms": trav_ms},
             "e2e": {"value": e2e, "unit": "packets/s", "h2d_bytes_per_step": len(phases) * (4 * nl + 64),
-                    "d2h_bytes_per_step": cubes_bytes},
+                    "d2h_bytes_per_step": cubes_bytes, "steps": e2e_steps},
             # per wave: the event pass, the scatter-and-launch pass and the two traversal kernels
             # (path jobs, peel-off jobs)
             "gpu_launches": 4 * waves * len(phases) * args.steps,
@@ -503,7 +563,7 @@ def cpu_baseline(args, wl, ctx):
     model = wl.model
     model.rho = ctx.density()
     threads = os.cpu_count() or 1
-    kw = dict(dust_emission_phase=wl.dust_phase)
+    kw = dict(dust_emission_phase=wl.dust_phase, selfabs_cycles=wl.selfabs_cycles)
     probe = oracle.simulate(model, args.packets, nthreads=threads, seed=1, max_packets=2000, **kw)
     rate = probe["stats"]["packets"] / max(probe["stats"]["seconds"], 1e-6)
     sample = int(max(1000, min(5e6, rate * args.cpu_seconds)))
@@ -512,7 +572,7 @@ def cpu_baseline(args, wl, ctx):
     return {"value": r["stats"]["packets"] / r["stats"]["seconds"], "unit": "packets/s", "cores": threads,
             "kind": "port", "sample": "%d packets over all %d wavelengths%s (%.1f s of packet loops)" %
                                       (r["stats"]["packets"], model.wavelengthGrid.Nlambda,
-                                       ", both phases" if wl.dust_phase else "", r["stats"]["seconds"])}
+                                       ", all phases" if wl.dust_phase else "", r["stats"]["seconds"])}
 
 
 if __name__ == "__main__":

@@ -35,13 +35,13 @@ extern "C" {
 /* ---- status codes ------------------------------------------------------------------ */
 #define SKG_OK                 0
 #define SKG_ERR_INVALID        1   /* invalid scene / argument (FatalError at setup in the reference) */
-#define SKG_ERR_OOM            2   /* device allocation failed */
+#define SKG_ERR_OOM            2   /* device allocation failed (the context or batch stays usable) */
 #define SKG_ERR_CUDA           3   /* CUDA runtime error */
 #define SKG_ERR_STEP_BUDGET    4   /* a packet exceeded its traversal-step or scattering budget */
 #define SKG_ERR_NAN_TAU        5   /* optical depth along a path is not a positive number (DustSystem.cpp:953-955) */
 #define SKG_ERR_TIMEOUT        6   /* a bounded host wait gave up */
 #define SKG_ERR_NO_DEVICE      7   /* no CUDA device */
-#define SKG_ERR_CAPACITY       8   /* an output buffer is too small (skg_trace_paths) */
+#define SKG_ERR_CAPACITY       8   /* an output buffer or a batch's tables are too small */
 #define SKG_ERR_BAD_CELL       9   /* a cell index out of range was produced or given */
 
 /* ---- enumerations ------------------------------------------------------------------ */
@@ -332,13 +332,61 @@ int  skg_batch_destroy(skg_batch* b);
    FP64 atomics.  With SKG_BATCH_GRAPH in `flags` the launch sequence (table uploads, counter
    reset, tracer) is captured once into a CUDA graph and replayed while the grid type and launch
    configuration stay the same.  Returns once enqueued on `stream` (NULL = the batch's own
-   stream). */
+   stream).  More work items, distinct simulations or wavelength entries than the batch was
+   created for return SKG_ERR_CAPACITY. */
 #define SKG_BATCH_GRAPH 1
 int  skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, const skg_run_opts* opts,
                    int flags, void* stream);
 int  skg_batch_sync(skg_batch* b, int timeout_ms);
 int  skg_batch_counters(skg_batch* b, skg_counters* out);
 int  skg_batch_last_ms(skg_batch* b, float* ms);
+
+/* ---- serving: continuous batching of many simulations on one device --------------------- */
+/* The request pattern of FitSKIRT (FitSKIRTcore/OligoFitScheme.cpp:123-149 runs one simulation per
+   parameter set through AdjustableSkirtSimulation::performWith, AdjustableSkirtSimulation.cpp:
+   145-194): many short simulations of one ski file with a few values substituted.  A server admits
+   submitted requests in arrival order while a batch slot is free and the request's device-memory
+   bound fits hbm_budget (admission by HBM footprint), builds their contexts on a host thread of
+   its own, and runs ticks -- one batched launch (skg_batch_run) carrying the next packet slice of
+   every admitted request, oldest first up to tick_budget packets -- so that requests arriving
+   while others run join the next tick.  A request retires when all its packets have run: its
+   instrument's tallies are copied into the caller's buffers and its context is freed.  Its
+   packets draw from streams keyed by its seed and packet index, so its result equals the same
+   simulation run alone (skg_run_phase with count = npp) up to the order of the FP64 tally
+   additions.  The stellar emission phase is served. */
+typedef struct skg_server skg_server;
+typedef struct skg_server_opts {
+    int64_t hbm_budget;                     /* device bytes the admitted requests may hold together (0: 40 GiB) */
+    int32_t max_slots;                      /* requests per launch, 1..64 (0: 64) */
+    int64_t tick_packets;                   /* packets per wavelength a request runs per tick at most (0: 2^22) */
+    int64_t tick_budget;                    /* packets (all wavelengths) one tick hands out (0: 48 * 2^20) */
+    int32_t precision;                      /* SKG_PREC_* of the traversal geometry */
+} skg_server_opts;
+typedef struct skg_request {
+    const skg_scene* scene;                 /* copied by skg_submit, arrays included */
+    const int32_t* ells;                    /* wavelength indices (1..64 of them) */
+    int32_t nell;
+    uint64_t packages;                      /* packets per wavelength (the simulation's Npp) */
+    uint64_t seed;
+    int32_t instr;                          /* the instrument whose tallies are the result */
+    double* cube;                           /* host buffer of the cube length (skg_scene_tally_sizes), or NULL */
+    double* sed;                            /* host buffer of the SED length, or NULL; both written by the
+                                               server thread, and final once skg_poll returns SKG_OK */
+} skg_request;
+int  skg_server_create(int device, const skg_server_opts* opts, skg_server** out);
+/* Queues a request; returns at once with its id. */
+int  skg_submit(skg_server* s, const skg_request* req, int64_t* id);
+/* Waits up to timeout_ms (-1: no limit) for request id: SKG_ERR_TIMEOUT while it runs, else its
+   status (SKG_OK: the result is in its buffers), reported once; latency_s (optional) receives the
+   time from submission to completion. */
+int  skg_poll(skg_server* s, int64_t id, int timeout_ms, double* latency_s);
+/* Ticks run, requests completed, packets run (all wavelengths) and the device time of the ticks. */
+int  skg_server_stats(skg_server* s, int64_t* ticks, int64_t* completed, int64_t* packets, double* tick_ms);
+/* Waits for a context being built, ends every unfinished request with SKG_ERR_INVALID (its buffers
+   are not written), and frees the server. */
+int  skg_server_destroy(skg_server* s);
+/* Tally lengths of instrument instr of a scene (as skg_tally_sizes gives for its context). */
+int  skg_scene_tally_sizes(const skg_scene* scene, int instr, int64_t* cube_len, int64_t* sed_len);
 
 /* Zeroes all tallies (instrument cubes and SEDs, absorbed luminosity). */
 int  skg_reset_tallies(skg_ctx* ctx);

@@ -66,17 +66,48 @@ struct Box {
 };
 
 // ---------------------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11), the counter-based generator of the library's
+// device kernels, restated for the checks that need the device's samples (tree node masses) or
+// streams keyed by packet (packet-range runs): key = seed, counter words = (block, node id lo, node id hi,
+// stream), deviates ((u32 + 0.5) * 2^-32).
+struct Philox {
+    uint32_t k0 = 0, k1 = 0, c1 = 0, c2 = 0, c3 = 0, c0 = 0, b[4] = {0, 0, 0, 0}; int left = 0;
+    Philox() = default;
+    Philox(uint64_t seed, uint64_t id, uint32_t stream)
+        : k0((uint32_t)seed), k1((uint32_t)(seed >> 32)), c1((uint32_t)id), c2((uint32_t)(id >> 32)), c3(stream) {}
+    double uniform() {
+        if (left == 0) {
+            uint32_t x0 = c0, x1 = c1, x2 = c2, x3 = c3, a = k0, bb = k1;
+            for (int r = 0; r < 10; r++) {
+                uint64_t p0 = (uint64_t)0xD2511F53u * x0, p1 = (uint64_t)0xCD9E8D57u * x2;
+                uint32_t y0 = (uint32_t)(p1 >> 32) ^ x1 ^ a, y1 = (uint32_t)p1;
+                uint32_t y2 = (uint32_t)(p0 >> 32) ^ x3 ^ bb, y3 = (uint32_t)p0;
+                x0 = y0; x1 = y1; x2 = y2; x3 = y3;
+                a += 0x9E3779B9u; bb += 0xBB67AE85u;
+            }
+            b[0] = x0; b[1] = x1; b[2] = x2; b[3] = x3; left = 4; c0++;
+        }
+        return ((double)b[4 - (left--)] + 0.5) * 2.3283064365386963e-10;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
 // Random (SKIRTcore/Random.cpp): one MT19937 state per thread, seeded seed+thread (:41-56),
 // uniform deviates excluding 0 and 1 (:90-127).
 
 struct Rng {
     unsigned long mt[624];
     int mti;
+    // packet-range runs draw from a counter-based stream keyed by the packet instead of the
+    // thread's MT19937 stream (orc_simulate_packets)
+    bool counter = false;
+    Philox ph;
     void init(unsigned long seed) {            // Random.cpp:46-50
         mt[0] = seed & 0xffffffffUL;
         for (mti = 1; mti < 624; mti++) mt[mti] = (69069UL * mt[mti-1]) & 0xffffffffUL;
     }
     double uniform() {                          // Random.cpp:90-127
+        if (counter) return ph.uniform();
         static const unsigned long mag01[2] = {0x0UL, 0x9908b0dfUL};
         double ans;
         do {
@@ -1328,29 +1359,6 @@ static void sampleDensity(Sim& S, int Nrandom, int nthreads, uint64_t seed) {
 // (BinTreeNode.cpp:40-77: two boxes split at the middle along direction level % 3).  Nodes are
 // visited in creation order; children are appended, so the ids follow the reference's.
 
-// Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11), restated to reproduce the library's
-// device sampler of node masses: key = seed, counter words = (block, node id lo, node id hi,
-// stream), deviates ((u32 + 0.5) * 2^-32).
-struct Philox {
-    uint32_t k0, k1, c1, c2, c3, c0 = 0, b[4]; int left = 0;
-    Philox(uint64_t seed, uint64_t id, uint32_t stream)
-        : k0((uint32_t)seed), k1((uint32_t)(seed >> 32)), c1((uint32_t)id), c2((uint32_t)(id >> 32)), c3(stream) {}
-    double uniform() {
-        if (left == 0) {
-            uint32_t x0 = c0, x1 = c1, x2 = c2, x3 = c3, a = k0, bb = k1;
-            for (int r = 0; r < 10; r++) {
-                uint64_t p0 = (uint64_t)0xD2511F53u * x0, p1 = (uint64_t)0xCD9E8D57u * x2;
-                uint32_t y0 = (uint32_t)(p1 >> 32) ^ x1 ^ a, y1 = (uint32_t)p1;
-                uint32_t y2 = (uint32_t)(p0 >> 32) ^ x3 ^ bb, y3 = (uint32_t)p0;
-                x0 = y0; x1 = y1; x2 = y2; x3 = y3;
-                a += 0x9E3779B9u; bb += 0xBB67AE85u;
-            }
-            b[0] = x0; b[1] = x1; b[2] = x2; b[3] = x3; left = 4; c0++;
-        }
-        return ((double)b[4 - (left--)] + 0.5) * 2.3283064365386963e-10;
-    }
-};
-
 struct TreeBuild {
     vector<Box> box; vector<int> child, father, level; vector<int8_t> dir; vector<uint8_t> split;
     void split_node(int l, int type) {
@@ -1617,16 +1625,73 @@ int orc_tree_build(const skg_scene* sc, int type, int minlevel, int maxlevel, do
     return 0;
 }
 
+
+// The stellar emission phase for the packets [first, first+count) of every listed wavelength of a
+// simulation of npp packets per wavelength (each carrying L_ell/npp), every packet drawing from its
+// own counter-based stream keyed by (seed, packet id, wavelength): the tallies of any partition of
+// [0, npp) into ranges sum to those of the whole range, up to the order of the FP64 additions --
+// the reference's MPI task mode (MonteCarloSimulation.cpp:98-104) with a deterministic split.
+// Needs scene->rho.
+int orc_simulate_packets(const skg_scene* sc, uint64_t npp, uint64_t first, uint64_t count, int nthreads,
+                         uint64_t seed, const int32_t* ells, int nell, double** cubes, double** seds,
+                         double* labs_stel, orc_stats* st) {
+    if (!sc->rho) { g_err = "orc_simulate_packets needs scene->rho"; return SKG_ERR_INVALID; }
+    Sim* S = buildSim(sc);
+    Sim& R = *S;
+    const size_t nc = R.grid->ncells;
+    R.rho.assign(sc->rho, sc->rho + nc*R.ncomp);
+    vector<int> ellv;
+    if (ells && nell > 0) ellv.assign(ells, ells + nell); else for (int e = 0; e < R.nlambda; e++) ellv.push_back(e);
+    const uint64_t B = 1024, nblk = (count + B - 1)/B, nitems = ellv.size()*nblk;
+    std::atomic<uint64_t> next{0};
+    const auto t0 = std::chrono::steady_clock::now();
+    auto worker = [&]() {
+        Rng rng; rng.counter = true;
+        Packet pp; Path path, ppath;
+        uint64_t it;
+        while ((it = next.fetch_add(1)) < nitems) {
+            const int ell = ellv[it/nblk];
+            const double L = R.Lv[ell]/npp;
+            if (!(L > 0)) continue;
+            const uint64_t b0 = first + (it % nblk)*B, b1 = std::min(first + count, b0 + B);
+            for (uint64_t id = b0; id < b1; id++) {
+                rng.ph = Philox(seed, id, 0xC0DE0000u + (uint32_t)ell);
+                stellarLaunch(R, pp, ell, L, rng);
+                R.stats.packets++;
+                if (pp.L > 0) lifecycle(R, pp, path, ppath, rng, L/R.minWeightReduction, R.storeAbs, true);
+            }
+        }
+    };
+    vector<std::thread> th;
+    for (int t = 1; t < nthreads; t++) th.emplace_back(worker);
+    worker();
+    for (auto& t : th) t.join();
+    for (int i = 0; i < sc->ninstr; i++) {
+        if (cubes && cubes[i] && !R.instr[i].cube.empty())
+            std::memcpy(cubes[i], R.instr[i].cube.data(), R.instr[i].cube.size()*sizeof(double));
+        if (seds && seds[i]) std::memcpy(seds[i], R.instr[i].sed.data(), R.instr[i].sed.size()*sizeof(double));
+    }
+    if (labs_stel) std::memcpy(labs_stel, R.LabsStel.data(), nc*R.nlambda*sizeof(double));
+    if (st) {
+        st->packets = R.stats.packets; st->steps = R.stats.steps; st->traversals = R.stats.traversals;
+        st->scatterings = R.stats.scatterings; st->fallbacks = R.stats.fallbacks; st->npp = npp; st->chunks = nitems;
+        st->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    delete R.grid; delete S;
+    return 0;
+}
+
 // Runs a simulation: the stellar emission phase (MonteCarloSimulation::runstellaremission,
 // MonteCarloSimulation.cpp:241-295) for `packages` per wavelength, optionally followed by
-// `selfabs_cycles` dust self-absorption cycles (fixed cycle count, PanMonteCarloSimulation.cpp:106-242,
-// one stage) and the dust emission phase (:246-346).  If max_packets > 0 only that many
+// `selfabs_cycles` dust self-absorption cycles (a fixed cycle count: at `packages` in one stage, or,
+// with selfabs_staged, in each of the reference's three stages, PanMonteCarloSimulation.cpp:106-187)
+// and the dust emission phase (:246-346).  If max_packets > 0 only that many
 // packets of each phase run (a bounded sample for timing); Npp is unchanged so that the
 // per-packet luminosity stays that of the full run.  st->seconds is the time of the packet loops
 // of the phases (as the reference's TimeLogger times a phase), without the set-up.
 // cubes[i]/seds[i] receive instrument i's tallies (layout of skg_read_instrument).
 int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t seed, int selfabs_cycles,
-                 int dust_emission_phase, int64_t max_packets, const int32_t* ells, int nell,
+                 int selfabs_staged, int dust_emission_phase, int64_t max_packets, const int32_t* ells, int nell,
                  double** cubes, double** seds,
                  double* labs_stel, double* labs_dust, double* temperature, orc_stats* st) {
     Sim* S = buildSim(sc);
@@ -1641,7 +1706,7 @@ int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t se
     if (ells && nell > 0) ellv.assign(ells, ells + nell); else for (int e = 0; e < nl; e++) ellv.push_back(e);
     const int nsel = (int)ellv.size();
     uint64_t Nchunks, chunksize, Npp;
-    chunkParams(packages, nthreads, 1, nl, Nchunks, chunksize, Npp);
+    chunkParams(packages, nthreads, 1, nsel, Nchunks, chunksize, Npp);   // chunks over the wavelengths run
     std::atomic<int64_t> launched{0};
     double loop_seconds = 0;
     const auto t_loop = std::chrono::steady_clock::now();
@@ -1663,7 +1728,9 @@ int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t se
     loop_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t_loop).count();
 
     // dust self-absorption cycles and dust emission (PanMonteCarloSimulation.cpp:106-346)
+    int dust_phases = 0;
     auto dustPhase = [&](double pk, bool selfabs) {
+        const uint64_t phase_seed = seed + 7919*(uint64_t)(++dust_phases);
         calcDustEmission(R);
         if (selfabs) std::fill(R.LabsDust.begin(), R.LabsDust.end(), 0.0);   // rebootLabsdust
         uint64_t nch, csz, npp;
@@ -1683,7 +1750,7 @@ int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t se
         }
         std::atomic<int64_t> emitted{0};
         const auto t_dust = std::chrono::steady_clock::now();
-        parallelCall(nthreads, (uint64_t)nl*nch, seed + 7919*(selfabs ? 1 : 2), [&](uint64_t index, Rng& rng) {
+        parallelCall(nthreads, (uint64_t)nl*nch, phase_seed, [&](uint64_t index, Rng& rng) {
             int ell = index % nl;
             double Ltot = Ltots[ell];
             if (!(Ltot > 0)) return;
@@ -1711,7 +1778,15 @@ int orc_simulate(const skg_scene* sc, double packages, int nthreads, uint64_t se
         loop_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t_dust).count();
     };
     if (R.dustEmission && R.ncomp && !R.Tv.empty()) {
-        for (int c = 0; c < selfabs_cycles; c++) dustPhase(packages, true);
+        if (selfabs_staged) {
+            // rundustselfabsorption with a fixed cycle count (PanMonteCarloSimulation.cpp:106-187):
+            // three stages of that many cycles with 1/10, 1/3 and 1 times the packages
+            const double factor[3] = {1./10., 1./3., 1.};
+            for (int stage = 0; stage < 3; stage++)
+                for (int c = 0; c < selfabs_cycles; c++) dustPhase(packages*factor[stage], true);
+        } else {
+            for (int c = 0; c < selfabs_cycles; c++) dustPhase(packages, true);
+        }
         if (dust_emission_phase) dustPhase(packages, false);
     }
 

@@ -80,14 +80,52 @@ def lib():
         L.orc_sample_density.argtypes = [C.c_void_p, C.c_int, C.c_uint64, dp]
         L.orc_chunk_params.argtypes = [C.c_double, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint64),
                                        C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.orc_simulate_packets.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_int, C.c_uint64, i32p,
+                                           C.c_int, C.POINTER(dp), C.POINTER(dp), dp, C.POINTER(Stats)]
         L.orc_tree_build.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_uint64, C.c_int,
                                      C.c_int, C.c_int64, C.POINTER(C.c_uint8), dp, i32p, i32p, i32p,
                                      C.POINTER(C.c_int8), i32p, i64p]
-        L.orc_simulate.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_int64, i32p,
+        L.orc_simulate.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int64, i32p,
                                    C.c_int,
                                    C.POINTER(dp), C.POINTER(dp), dp, dp, dp, C.POINTER(Stats)]
         _lib = L
     return _lib
+
+
+def _tallies(model):
+    nl = model.wavelengthGrid.Nlambda
+    cubes, seds = [], []
+    for ins in model.instruments:
+        nc = 1 if ins.type != 3 else 6 + ins.scatteringLevels
+        if ins.type == 1 and getattr(ins, "writeStellarComps", False):
+            nc = 1 + len(model.stellarComps)
+        cubes.append(None if ins.type == 0 else np.zeros((nc, nl, ins.pixelsY, ins.pixelsX)))
+        seds.append(np.zeros((nc, nl)))
+    ni = len(model.instruments)
+    cp = (dp * max(ni, 1))()
+    sp = (dp * max(ni, 1))()
+    for i in range(ni):
+        cp[i] = cubes[i].ctypes.data_as(dp) if cubes[i] is not None else None
+        sp[i] = seds[i].ctypes.data_as(dp)
+    return cubes, seds, cp, sp
+
+
+def simulate_packets(model, npp, first, count, nthreads=8, seed=4357, ells=None):
+    """The stellar phase for packets [first, first+count) of a simulation of npp packets per
+    wavelength, every packet on its own counter-based stream (orc_simulate_packets): tallies of
+    disjoint ranges sum to those of their union.  Needs model.rho."""
+    assert model.rho is not None
+    sc, keep = model.lower()
+    cubes, seds, cp, sp = _tallies(model)
+    nl = model.wavelengthGrid.Nlambda
+    labs = np.zeros(model.dustGrid.ncells * nl)
+    ev = np.ascontiguousarray(ells if ells is not None else [], dtype=np.int32)
+    st = Stats()
+    assert lib().orc_simulate_packets(C.byref(sc), int(npp), int(first), int(count), nthreads, seed,
+                                      ev.ctypes.data_as(i32p) if len(ev) else None, len(ev), cp, sp,
+                                      labs.ctypes.data_as(dp), C.byref(st)) == 0
+    return dict(cubes=cubes, seds=seds, labs_stel=labs.reshape(-1, nl),
+                stats={n: getattr(st, n) for n, _ in Stats._fields_})
 
 
 def trace_paths(model, r, k, nthreads=None):
@@ -136,9 +174,11 @@ def sample_density(model, nthreads=8, seed=99):
 
 
 def simulate(model, packages, nthreads=8, seed=4357, selfabs_cycles=0, dust_emission_phase=False, max_packets=0,
-             ells=None):
+             ells=None, selfabs_staged=False):
     """Runs the restated life cycle; returns dict(cubes, seds, labs_stel, labs_dust, T, stats).
-    ells: run the stellar phase for these wavelength indices only (default: all)."""
+    ells: run the stellar phase for these wavelength indices only (default: all).  selfabs_cycles
+    self-absorption cycles at `packages`, or with selfabs_staged in each of the reference's three
+    stages (1/10, 1/3 and 1 times the packages)."""
     sc, keep = model.lower()
     nl = model.wavelengthGrid.Nlambda
     ncomp = []
@@ -165,7 +205,8 @@ def simulate(model, packages, nthreads=8, seed=4357, selfabs_cycles=0, dust_emis
     T = np.zeros(max(ncells, 1))
     st = Stats()
     ev = np.ascontiguousarray(ells if ells is not None else [], dtype=np.int32)
-    assert lib().orc_simulate(C.byref(sc), float(packages), nthreads, seed, selfabs_cycles, int(dust_emission_phase),
+    assert lib().orc_simulate(C.byref(sc), float(packages), nthreads, seed, selfabs_cycles, int(selfabs_staged),
+                              int(dust_emission_phase),
                               int(max_packets), ev.ctypes.data_as(i32p) if len(ev) else None, len(ev), cp, sp, ls.ctypes.data_as(dp), ld.ctypes.data_as(dp),
                               T.ctypes.data_as(dp), C.byref(st)) == 0
     stats = {n: getattr(st, n) for n, _ in Stats._fields_}
@@ -232,3 +273,53 @@ def tree_build(model, gtype, extent, minLevel=2, maxLevel=6, maxMassFraction=1e-
         search = A.SEARCH_NEIGHBOR
     grid = TreeDustGrid(gtype, tuple(extent), box[: 6 * n], child[:n], father[:n], cell[:n], d[:n], off, ids, search)
     return grid, split[:n], lev[:n]
+
+
+def voronoi_mesh(sites, extent):
+    """The tessellation by Voro++ (oracle/_ref) with the block lists of VoronoiMesh::buildMesh
+    (VoronoiMesh.cpp:330-395: nb = max(3, min(1000, 3 N^(1/3))) blocks per axis, each listing the
+    cells whose box, widened by eps, overlaps it)."""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, ".."))
+    from skirt7_b200 import _abi as A
+    from skirt7_b200.scene import VoronoiDustGrid
+    EXT = tuple(extent)
+    R = ref()
+    assert R is not None, "Voro++ (oracle/_ref) not built"
+    n = len(sites)
+    nb = max(3, min(1000, int(3.0 * n ** (1.0 / 3.0))))
+    e = np.ascontiguousarray(EXT, dtype=np.float64)
+    s = np.ascontiguousarray(sites, dtype=np.float64)
+    off = np.zeros(n + 1, dtype=np.int64)
+    vol, cen, bb = np.zeros(n), np.zeros(3 * n), np.zeros(6 * n)
+    cap = 20 * n
+    while True:
+        ids = np.zeros(cap, dtype=np.int32)
+        q = R.ref_voronoi(s.ctypes.data_as(dp), n, e.ctypes.data_as(dp), nb, off.ctypes.data_as(A.i64p),
+                          ids.ctypes.data_as(A.i32p), cap, vol.ctypes.data_as(dp), cen.ctypes.data_as(dp),
+                          bb.ctypes.data_as(dp))
+        if q >= 0:
+            break
+        cap = -q
+    ids = ids[: off[-1]]
+    bb = bb.reshape(n, 6)
+    lo, hi = np.array(EXT[:3]), np.array(EXT[3:])
+    eps = 1e-12 * np.linalg.norm(hi - lo)
+
+    def idx(p):   # Box::cellindices (Box.hpp:120-125)
+        return np.clip((nb * (p - lo) / (hi - lo)).astype(np.int64), 0, nb - 1)
+
+    i1, i2 = idx(bb[:, :3] - eps), idx(bb[:, 3:] + eps)
+    span = i2 - i1 + 1
+    cnt = span.prod(1)
+    cell = np.repeat(np.arange(n), cnt)
+    t = np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+    sy, sz = np.repeat(span[:, 1], cnt), np.repeat(span[:, 2], cnt)
+    bi = np.repeat(i1[:, 0], cnt) + t // (sy * sz)
+    bj = np.repeat(i1[:, 1], cnt) + (t // sz) % sy
+    bk = np.repeat(i1[:, 2], cnt) + t % sz
+    block = (bi * nb + bj) * nb + bk
+    order = np.argsort(block, kind="stable")
+    boff = np.zeros(nb ** 3 + 1, dtype=np.int64)
+    boff[1:] = np.cumsum(np.bincount(block, minlength=nb ** 3))
+    return VoronoiDustGrid(EXT, s, off, ids, nb, boff, cell[order].astype(np.int32), vol, bb)

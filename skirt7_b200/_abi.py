@@ -120,6 +120,16 @@ class Work(C.Structure):
 
 BATCH_GRAPH = 1
 
+
+class ServerOpts(C.Structure):
+    _fields_ = [("hbm_budget", C.c_int64), ("max_slots", C.c_int32), ("tick_packets", C.c_int64),
+                ("tick_budget", C.c_int64), ("precision", C.c_int32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("scene", C.POINTER(Scene)), ("ells", i32p), ("nell", C.c_int32), ("packages", C.c_uint64),
+                ("seed", C.c_uint64), ("instr", C.c_int32), ("cube", dp), ("sed", dp)]
+
 # exported functions: name -> (restype, argtypes)
 FUNCS = {
     "skg_version": (C.c_int, []),
@@ -170,6 +180,12 @@ FUNCS = {
     "skg_voronoi_arrays": (C.c_int, [C.c_void_p, dp, i64p, i32p, dp, dp, dp, i64p, i32p]),
     "skg_voronoi_grid": (C.c_int, [C.c_void_p, C.POINTER(Grid)]),
     "skg_voronoi_destroy": (C.c_int, [C.c_void_p]),
+    "skg_server_create": (C.c_int, [C.c_int, C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]),
+    "skg_submit": (C.c_int, [C.c_void_p, C.POINTER(Request), i64p]),
+    "skg_poll": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, dp]),
+    "skg_server_stats": (C.c_int, [C.c_void_p, i64p, i64p, i64p, dp]),
+    "skg_server_destroy": (C.c_int, [C.c_void_p]),
+    "skg_scene_tally_sizes": (C.c_int, [C.POINTER(Scene), C.c_int, i64p, i64p]),
 }
 
 _lib = None

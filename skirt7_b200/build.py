@@ -25,7 +25,7 @@ UNITS = [
     ("skg_voronoi.cu", []),
     ("skg_api.cu", []),
 ]
-CXX_UNITS = ["skg_host.cpp"]
+CXX_UNITS = ["skg_host.cpp", "skg_serve.cpp"]
 
 
 def _run(cmd):
@@ -63,9 +63,10 @@ def build(verbose=False, ptxas_info=False):
         o = os.path.join(BUILD, src + ".o")
         objs.append(o)
         if _stale(o, [s, __file__] + headers):
-            _run(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I" + CUDA_INC, "-c", "-o", o, s])
+            _run(["g++", "-O2", "-std=c++17", "-fPIC", "-pthread", "-ffp-contract=off", "-I" + CUDA_INC, "-c", "-o", o,
+                  s])
     if _stale(LIB, objs):
-        _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
+        _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-Xcompiler", "-pthread"])
     return LIB
 
 

@@ -46,7 +46,12 @@ struct Allocs {
 };
 
 struct Failure { int code; std::string msg; };
-#define CK(expr) do { cudaError_t e_ = (expr); if (e_ != cudaSuccess) throw Failure{SKG_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)}; } while (0)
+// A failed call throws its status: SKG_ERR_OOM for an allocation the device cannot satisfy (a
+// non-sticky error, cleared here so that the context stays usable), SKG_ERR_CUDA otherwise.
+#define CK(expr) do { cudaError_t e_ = (expr); if (e_ != cudaSuccess) {                          \
+        if (e_ == cudaErrorMemoryAllocation) cudaGetLastError();                                  \
+        throw Failure{e_ == cudaErrorMemoryAllocation ? SKG_ERR_OOM : SKG_ERR_CUDA,                \
+                      std::string(#expr) + ": " + cudaGetErrorString(e_)}; } } while (0)
 #define REQUIRE(cond, msg) do { if (!(cond)) throw Failure{SKG_ERR_INVALID, msg}; } while (0)
 
 template<typename T> T* upload(Allocs& A, const T* h, size_t n, cudaStream_t s) {
@@ -1199,7 +1204,8 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
     try {
         CK(cudaSetDevice(b->device));
         REQUIRE(phase >= SKG_PHASE_STELLAR && phase <= SKG_PHASE_DUST_EMISSION, "unknown phase");
-        REQUIRE(nwork >= 0 && nwork <= b->T.max_items, "too many work items for this batch");
+        REQUIRE(nwork >= 0, "negative work item count");
+        if (nwork > b->T.max_items) throw Failure{SKG_ERR_CAPACITY, "more work items than the batch was created for"};
         cudaStream_t s = stream ? (cudaStream_t)stream : b->stream;
         // the pinned tables may still be read by the previous launch's copies
         CK(cudaEventSynchronize(b->copied));
@@ -1222,7 +1228,7 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
             int slot = -1;
             for (int q = 0; q < nslots; q++) if (slots[q] == w.ctx) slot = q;
             if (slot < 0) {
-                REQUIRE(nslots < b->T.max_slots, "too many distinct simulations for this batch");
+                if (!(nslots < b->T.max_slots)) throw Failure{SKG_ERR_CAPACITY, "too many distinct simulations for this batch"};
                 slot = nslots++;
                 slots.push_back(w.ctx);
                 DevGrid g = w.ctx->grid;
@@ -1230,7 +1236,7 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
                 b->h_grids[slot] = g;
                 b->h_scenes[slot] = w.ctx->ds;
             }
-            REQUIRE(nells + w.nell <= b->T.max_ells, "too many wavelength entries for this batch");
+            if (!(nells + w.nell <= b->T.max_ells)) throw Failure{SKG_ERR_CAPACITY, "too many wavelength entries for this batch"};
             WorkItem& W = b->h_items[i];
             std::memset(&W, 0, sizeof(W));
             W.slot = slot; W.nell = w.nell; W.ell0 = nells; W.npp_total = w.npp; W.first = w.first; W.count = w.count;

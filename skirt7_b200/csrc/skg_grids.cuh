@@ -289,6 +289,11 @@ struct CartStepperRef {
 
 template<typename R> struct CartStepper : CartStepperRef<R> {};
 
+// FP32 Cartesian cell step without a branch per crossed axis (1) or with the three branches (0)
+#ifndef SKG_CART_SELECT
+#define SKG_CART_SELECT 1
+#endif
+
 // FP32 production walk of the Cartesian grid: after the reference's entry (nudge and cell
 // location), a DDA over the ray parameter t measured from the entry point.  The next wall of each
 // axis sits at t = (plane - origin) / k, computed once per crossing with a reciprocal taken once per
@@ -332,6 +337,42 @@ struct CartStepper<float> : CartStepperRef<float> {
         if (pd.pop(ds)) { m = -1; return true; }
         return walk(g, m, ds);
     }
+#if SKG_CART_SELECT
+    // One cell step as a single instruction stream: the crossed axis is an index and every
+    // per-axis quantity a select, so lanes of a warp that cross different axes do not split into
+    // three branches.  The crossed axis is the one of the three branches of the reference's tie
+    // order (x if tx <= ty and tx <= tz, else y if ty <= tz, else z: for the non-NaN parameters of
+    // a started walk the same choice), and every value is computed as in those branches.
+    SKG_D bool walk(const DevGrid& g, int& m, float& ds) {
+        while (!done) {
+            if (++steps > g.max_steps) { done = true; return false; }
+            m = k + g.nz * j + g.nz * g.ny * i;
+            const int a = (tx <= ty && tx <= tz) ? 0 : (ty <= tz ? 1 : 2);
+            const float t = a == 0 ? tx : (a == 1 ? ty : tz);
+            if (t != t) { done = true; return false; }   // NaN direction
+            const float ka = a == 0 ? kx : (a == 1 ? ky : kz);
+            const int n = a == 0 ? g.nx : (a == 1 ? g.ny : g.nz);
+            const int q = (a == 0 ? i : (a == 1 ? j : k)) + ((ka < 0.f) ? -1 : 1);
+            if (a == 0) i = q;
+            if (a == 1) j = q;
+            if (a == 2) k = q;
+            if (q >= n || q < 0) done = true;
+            else {
+                const float* pl = a == 0 ? g.xvf : (a == 1 ? g.yvf : g.zvf);
+                const float o = a == 0 ? x : (a == 1 ? y : z);
+                const float u = a == 0 ? ux : (a == 1 ? uy : uz);
+                const float tn = (__ldg(pl + ((ka < 0.f) ? q : q + 1)) - o) * u;
+                if (a == 0) tx = tn;
+                if (a == 1) ty = tn;
+                if (a == 2) tz = tn;
+            }
+            const float d = t - tc;
+            tc = t;
+            if (d > 0.f) { ds = d; return true; }   // DustGridPath::addSegment drops ds <= 0
+        }
+        return false;
+    }
+#else
     SKG_D bool walk(const DevGrid& g, int& m, float& ds) {
         while (!done) {
             if (++steps > g.max_steps) { done = true; return false; }
@@ -359,6 +400,7 @@ struct CartStepper<float> : CartStepperRef<float> {
         }
         return false;
     }
+#endif
 };
 
 // =============================================================================================

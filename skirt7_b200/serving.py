@@ -302,3 +302,91 @@ def latency_stats(reqs):
     lat = np.array([r.latency for r in reqs])
     return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_s": float(lat.mean()), "max_s": float(lat.max()), "n": len(lat)}
+
+
+class NativeServer:
+    """The continuous-batching server of the C ABI (skg_server: skg_submit / skg_poll), whose loop
+    and context set-up run on native threads: the same admission, ticks and retirement as Server,
+    for a host program that links the library directly (a C++ FitSKIRT)."""
+
+    def __init__(self, device=0, hbm_budget=0, max_slots=0, tick_packets=0, tick_budget=0, precision=A.PREC_FP32):
+        import ctypes as C
+        self.lib = A.load()
+        o = A.ServerOpts(int(hbm_budget), int(max_slots), int(tick_packets), int(tick_budget), precision)
+        h = C.c_void_p()
+        A.check(self.lib.skg_server_create(device, C.byref(o), C.byref(h)))
+        self.h = h
+        self._out = {}
+
+    def submit(self, model, ells, packages, seed, instr=0):
+        """Queues one simulation (the scene is copied); returns its id."""
+        import ctypes as C
+        sc, keep = model.lower()
+        cl, sl = C.c_int64(), C.c_int64()
+        A.check(self.lib.skg_scene_tally_sizes(C.byref(sc), instr, C.byref(cl), C.byref(sl)))
+        cube = np.zeros(max(cl.value, 1))
+        sed = np.zeros(max(sl.value, 1))
+        e = np.ascontiguousarray(ells, dtype=np.int32)
+        q = A.Request(C.pointer(sc), e.ctypes.data_as(A.i32p), len(e), int(packages), int(seed), instr,
+                      cube.ctypes.data_as(A.dp) if cl.value else None, sed.ctypes.data_as(A.dp))
+        rid = C.c_int64()
+        A.check(self.lib.skg_submit(self.h, C.byref(q), C.byref(rid)))
+        ins = model.instruments[instr]
+        self._out[rid.value] = (cube, sed, cl.value, sl.value, model.wavelengthGrid.Nlambda, ins)
+        return rid.value
+
+    def poll(self, rid, timeout_ms=-1):
+        """(cube [components, nlambda, ny, nx] or None, sed [components, nlambda], latency s) once
+        request rid is done; raises SkirtError with SKG_ERR_TIMEOUT while it runs."""
+        import ctypes as C
+        lat = C.c_double()
+        A.check(self.lib.skg_poll(self.h, rid, int(timeout_ms), C.byref(lat)))
+        cube, sed, cl, sl, nl, ins = self._out.pop(rid)
+        ncomp = sl // nl
+        sed = sed[:sl].reshape(ncomp, nl)
+        cube = cube.reshape(ncomp, nl, ins.pixelsY, ins.pixelsX) if cl else None
+        return cube, sed, lat.value
+
+    def stats(self):
+        import ctypes as C
+        t, c, p, ms = C.c_int64(), C.c_int64(), C.c_int64(), C.c_double()
+        A.check(self.lib.skg_server_stats(self.h, C.byref(t), C.byref(c), C.byref(p), C.byref(ms)))
+        return {"ticks": t.value, "completed": c.value, "packets": p.value, "tick_device_s": ms.value / 1e3}
+
+    def close(self):
+        if self.h:
+            self.lib.skg_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def serve_native(requests, device=0, npix=256, realtime=True, **opts):
+    """Runs the request stream through NativeServer: each request is submitted at its arrival time
+    (realtime) and its frame polled; returns the requests with frame, admitted and done filled in
+    (done = arrival + the server's submission-to-completion latency)."""
+    srv = NativeServer(device=device, **opts)
+    pending = sorted(requests, key=lambda r: r.arrival)
+    ids = {}
+    t0 = time.perf_counter()
+    try:
+        for r in pending:
+            if realtime:
+                dt = r.arrival - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+            r.admitted = time.perf_counter() - t0
+            ids[r.rid] = srv.submit(build_model(r, npix), [0, 1, 2], r.packets, r.seed)
+        for r in pending:
+            cube, _, lat = srv.poll(ids[r.rid])
+            r.frame = cube[0]
+            r.done = r.admitted + lat
+        st = srv.stats()
+    finally:
+        srv.close()
+    st["makespan_s"] = time.perf_counter() - t0
+    return pending, st

@@ -48,6 +48,39 @@ VORONOI_SITES = 1000000
 VORONOI_SEED = 77
 
 
+class SubsetWavelengthGrid:
+    """Some wavelengths of a grid, with their own bin widths."""
+
+    def __init__(self, lambdav, dlambdav):
+        self.lambdav = np.ascontiguousarray(lambdav, dtype=np.float64)
+        self.dlambdav = np.ascontiguousarray(dlambdav, dtype=np.float64)
+
+    @property
+    def Nlambda(self):
+        return len(self.lambdav)
+
+
+def wavelength_subset(model, ells):
+    """The same simulation restricted to the wavelengths ells: stellar luminosities, mix tables and
+    bin widths of those wavelengths, the dust normalisation of the full model (its face-on optical
+    depth is defined at 0.55 micron of the full grid).  Packets of one wavelength never touch
+    another in the stellar phase, so these wavelengths of the full run and of this run have the
+    same expectation."""
+    import copy
+    from skirt7_b200.scene import DustComp, DustMix, StellarComp
+    model.normalise()
+    ells = list(ells)
+    sub = copy.copy(model)
+    wl = model.wavelengthGrid
+    sub.wavelengthGrid = SubsetWavelengthGrid(wl.lambdav[ells], wl.dlambdav[ells])
+    sub.stellarComps = [StellarComp(c.geometry, np.asarray(c.luminosities)[ells]) for c in model.stellarComps]
+    sub.dustComps = [DustComp(d.geometry, DustMix(np.asarray(d.mix.kappaext)[ells], np.asarray(d.mix.albedo)[ells],
+                                                  np.asarray(d.mix.asymmpar)[ells]), None, d.norm)
+                     for d in model.dustComps]
+    sub.instruments = list(model.instruments)
+    return sub
+
+
 def tree_hash(grid):
     h = hashlib.sha256()
     for a in (grid.node_box, grid.node_child, grid.node_cell):
@@ -99,10 +132,13 @@ def tree_grid(model, spec, nthreads=None):
 
 
 def octree_pan_model():
+    """Configuration 2's panchromatic disk: 50 wavelengths 0.1-10 micron, three 512x512 frames."""
     return models.pan_disk(nlambda=50, inclinations=(0, 60, 88), npix=512)
 
 
 def kdtree_point_model():
+    """Configuration 5's disk with a central point source (10 % of the luminosity): 100
+    wavelengths 0.1-1000 micron, a 512x512 frame at 60 degrees, absorption tallies kept."""
     return models.pan_disk(nlambda=100, lmin=0.1 * MICRON, lmax=1000 * MICRON, inclinations=(60,), npix=512,
                            point_fraction=0.1, write_absorption=True)
 
@@ -128,52 +164,15 @@ def voronoi_clumpy_model():
 
 
 def voropp_mesh(sites):
-    """The tessellation by Voro++ (oracle/_ref) with the block lists of VoronoiMesh::buildMesh
-    (VoronoiMesh.cpp:330-395: nb = max(3, min(1000, 3 N^(1/3))) blocks per axis, each listing the
-    cells whose box, widened by eps, overlaps it)."""
-    R = oracle.ref()
-    assert R is not None, "Voro++ (oracle/_ref) not built"
-    n = len(sites)
-    nb = max(3, min(1000, int(3.0 * n ** (1.0 / 3.0))))
-    e = np.ascontiguousarray(EXT, dtype=np.float64)
-    s = np.ascontiguousarray(sites, dtype=np.float64)
-    off = np.zeros(n + 1, dtype=np.int64)
-    vol, cen, bb = np.zeros(n), np.zeros(3 * n), np.zeros(6 * n)
-    cap = 20 * n
-    while True:
-        ids = np.zeros(cap, dtype=np.int32)
-        q = R.ref_voronoi(s.ctypes.data_as(dp), n, e.ctypes.data_as(dp), nb, off.ctypes.data_as(A.i64p),
-                          ids.ctypes.data_as(A.i32p), cap, vol.ctypes.data_as(dp), cen.ctypes.data_as(dp),
-                          bb.ctypes.data_as(dp))
-        if q >= 0:
-            break
-        cap = -q
-    ids = ids[: off[-1]]
-    bb = bb.reshape(n, 6)
-    lo, hi = np.array(EXT[:3]), np.array(EXT[3:])
-    eps = 1e-12 * np.linalg.norm(hi - lo)
-
-    def idx(p):   # Box::cellindices (Box.hpp:120-125)
-        return np.clip((nb * (p - lo) / (hi - lo)).astype(np.int64), 0, nb - 1)
-
-    i1, i2 = idx(bb[:, :3] - eps), idx(bb[:, 3:] + eps)
-    span = i2 - i1 + 1
-    cnt = span.prod(1)
-    cell = np.repeat(np.arange(n), cnt)
-    t = np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt)
-    sy, sz = np.repeat(span[:, 1], cnt), np.repeat(span[:, 2], cnt)
-    bi = np.repeat(i1[:, 0], cnt) + t // (sy * sz)
-    bj = np.repeat(i1[:, 1], cnt) + (t // sz) % sy
-    bk = np.repeat(i1[:, 2], cnt) + t % sz
-    block = (bi * nb + bj) * nb + bk
-    order = np.argsort(block, kind="stable")
-    boff = np.zeros(nb ** 3 + 1, dtype=np.int64)
-    boff[1:] = np.cumsum(np.bincount(block, minlength=nb ** 3))
-    return VoronoiDustGrid(EXT, s, off, ids, nb, boff, cell[order].astype(np.int32), vol, bb)
+    """The tessellation by Voro++ (oracle/_ref) with VoronoiMesh's block lists."""
+    return oracle.voronoi_mesh(sites, EXT)
 
 
-def block_sums(frame, f=32):
+def block_sums(frame, fmax=32):
+    """Sums over square blocks of pixels: the largest block size up to fmax that divides the frame
+    (32 for 512x512, 30 for 300x300)."""
     ny, nx = frame.shape[-2:]
+    f = next(d for d in range(fmax, 0, -1) if ny % d == 0 and nx % d == 0)
     return frame.reshape(frame.shape[:-2] + (ny // f, f, nx // f, f)).sum((-3, -1))
 
 

@@ -36,7 +36,8 @@ def test_exports_every_declared_symbol(lib):
 def test_struct_layout_matches_header():
     structs = {"skg_grid": A.Grid, "skg_geometry": A.Geometry, "skg_stellar_comp": A.StellarComp,
                "skg_dust_comp": A.DustComp, "skg_instrument": A.Instrument, "skg_scene": A.Scene,
-               "skg_run_opts": A.RunOpts, "skg_counters": A.Counters}
+               "skg_run_opts": A.RunOpts, "skg_counters": A.Counters, "skg_server_opts": A.ServerOpts,
+               "skg_request": A.Request, "skg_work": A.Work}
     src = '#include "%s"\n#include <stdio.h>\n#include <stddef.h>\nint main(){\n' % HDR
     for n in structs:
         src += 'printf("%s %%zu\\n", sizeof(%s));\n' % (n, n)
@@ -83,3 +84,26 @@ def test_invalid_scene_is_reported_not_thrown(lib):
     assert rc in (A.SKG_ERR_INVALID, A.SKG_ERR_NO_DEVICE)
     assert h.value is None
     assert lib.skg_last_error(None)
+
+
+def test_scene_tally_sizes_and_server_without_device(lib):
+    """skg_scene_tally_sizes gives the tally lengths of a scene's instruments before any context
+    exists (the serving caller's result buffers); without a device the server is refused cleanly."""
+    from skirt7_b200 import models
+    from skirt7_b200.scene import DEG, KPC, MPC, FullInstrument, FrameInstrument
+    m = models.oligo_disk(N=(8, 8, 4), npix=10, wavelengths=(0.45e-6, 0.55e-6))
+    m.instruments.append(FullInstrument(scatteringLevels=2, distance=10 * MPC, inclination=30 * DEG, pixelsX=6,
+                                        pixelsY=7, fieldOfViewX=40 * KPC, fieldOfViewY=40 * KPC, instrumentName="f"))
+    m.instruments.append(FrameInstrument(10 * MPC, 80 * DEG, 5, 4, 40 * KPC, 40 * KPC, instrumentName="c",
+                                         writeStellarComps=True))
+    sc, keep = m.lower()
+    want = [(1 * 2 * 10 * 10, 2), (0, 2), ((6 + 2) * 2 * 6 * 7, (6 + 2) * 2), (3 * 2 * 5 * 4, 3 * 2)]
+    for i, (c, s) in enumerate(want):
+        cl, sl = C.c_int64(), C.c_int64()
+        assert lib.skg_scene_tally_sizes(C.byref(sc), i, C.byref(cl), C.byref(sl)) == 0
+        assert (cl.value, sl.value) == (c, s), i
+    assert lib.skg_scene_tally_sizes(C.byref(sc), 4, None, None) == A.SKG_ERR_INVALID
+    from skirt7_b200 import runtime
+    if runtime.device_count() == 0:
+        h = C.c_void_p()
+        assert lib.skg_server_create(0, None, C.byref(h)) != 0 and not h.value

@@ -1,7 +1,9 @@
-"""The N>1 path on CPU with gloo ranks (world size 2): packet ranges are disjoint and cover the
-simulation, and the all-reduce of per-rank tallies reproduces the single-process result.  Tallies
-come from the oracle run on each rank's share of the packets, so the reduction is exercised on
-real frames; a deterministic additive stand-in checks exactness."""
+"""The N>1 path on CPU with gloo ranks: the packet ranges of skirt7_b200.distributed partition a
+simulation, and the all-reduce of the ranks' tallies (reduce_tallies) reproduces the single-process
+run.  Each rank runs the oracle's stellar phase on exactly its packet range (every packet on its
+own counter-based stream, oracle.simulate_packets), so the reduced frames, SEDs and absorbed
+luminosities must equal those of one process running all packets, up to the order of the FP64
+additions."""
 import os
 import socket
 
@@ -12,6 +14,8 @@ import torch.distributed as dist
 import torch.multiprocessing as mp
 
 from skirt7_b200.distributed import packet_range, reduce_tallies
+
+NPP = 3000
 
 
 @pytest.mark.parametrize("npp,world", [(10, 3), (1_000_000, 2), (7, 8), (1, 4), (0, 2)])
@@ -33,47 +37,58 @@ def _free_port():
     return p
 
 
-def _worker(rank, world, port, npp, out):
-    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
-    dist.init_process_group("gloo", rank=rank, world_size=world)
-    # additive stand-in for a phase: each packet id deposits a deterministic amount in a pixel
-    f, c = packet_range(npp, rank, world)
-    ids = np.arange(f, f + c)
-    frame = np.zeros((16, 16))
-    np.add.at(frame, (ids % 16, (ids * 7) % 16), 1.0 / (1 + ids))
-    t = torch.from_numpy(frame)
-    reduce_tallies([t])
-    # the oracle on this rank's share, reduced
+def _model():
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from helpers import cell_center_density
+    from skirt7_b200 import models
+    m = models.oligo_disk(N=(20, 20, 10), npix=24, with_sed=True)
+    m.rho = cell_center_density(m)
+    return m
+
+
+def _oracle():
     import sys
     sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
     import oracle
-    from skirt7_b200 import models
-    m = models.oligo_disk(N=(20, 20, 10), npix=20, with_sed=True)
-    r = oracle.simulate(m, 4000, nthreads=2, seed=11 + 1000 * rank, max_packets=c and 2000)
-    sed = torch.from_numpy(np.ascontiguousarray(r["seds"][1]))
-    reduce_tallies([sed])
+    return oracle
+
+
+def _worker(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    f, c = packet_range(NPP, rank, world)
+    r = _oracle().simulate_packets(_model(), NPP, f, c, nthreads=2, seed=99)
+    t = [torch.from_numpy(np.ascontiguousarray(r["cubes"][0])), torch.from_numpy(np.ascontiguousarray(r["seds"][1])),
+         torch.from_numpy(np.ascontiguousarray(r["labs_stel"]))]
+    reduce_tallies(t)
     if rank == 0:
-        out.put((t.numpy().copy(), sed.numpy().copy()))
+        out.put(([x.numpy().copy() for x in t], int(r["stats"]["packets"])))
     dist.barrier()
     dist.destroy_process_group()
 
 
-def test_gloo_reduction_matches_single_process():
-    npp, world = 5000, 2
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_reduction_matches_single_process(world):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    ps = [ctx.Process(target=_worker, args=(r, world, port, npp, q)) for r in range(world)]
+    ps = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
     for p in ps:
         p.start()
-    frame, sed = q.get(timeout=300)
+    (frame, sed, labs), _ = q.get(timeout=300)
     for p in ps:
         p.join(timeout=120)
         assert p.exitcode == 0
-    ids = np.arange(npp)
-    ref = np.zeros((16, 16))
-    np.add.at(ref, (ids % 16, (ids * 7) % 16), 1.0 / (1 + ids))
-    assert np.allclose(frame, ref, rtol=1e-14, atol=0)
-    # two half-runs of 2000 packets each, every packet carrying L/4000: the summed SED estimates the
-    # same flux as one run (within Monte Carlo noise)
-    assert sed[0, 0] > 0
+    whole = _oracle().simulate_packets(_model(), NPP, 0, NPP, nthreads=4, seed=99)
+    assert whole["stats"]["packets"] == NPP
+    for got, ref in ((frame, whole["cubes"][0]), (sed, whole["seds"][1]), (labs, whole["labs_stel"])):
+        assert ref.sum() > 0
+        assert np.allclose(got, ref, rtol=1e-11, atol=1e-14 * np.abs(ref).max())
+    # a different split of the same packets changes nothing either; a different seed does
+    half = [_oracle().simulate_packets(_model(), NPP, f, c, nthreads=2, seed=99) for f, c in ((0, 1000), (1000, 2000))]
+    assert np.allclose(half[0]["cubes"][0] + half[1]["cubes"][0], whole["cubes"][0], rtol=1e-11,
+                       atol=1e-14 * whole["cubes"][0].max())
+    other = _oracle().simulate_packets(_model(), NPP, 0, NPP, nthreads=4, seed=98)
+    assert not np.allclose(other["cubes"][0], whole["cubes"][0], rtol=1e-6)
