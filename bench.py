@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--workload", default="octree_pan", choices=WORKLOADS)
     p.add_argument("--packets", type=float, default=1e7, help="packets per wavelength per GPU per step")
     p.add_argument("--e2e-steps", type=int, default=5, help="steps of the end-to-end leg (at most --steps)")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="run with the library's default launch choices instead of the autotuner's (set-up, untimed)")
     p.add_argument("--max-level", type=int, default=10)
     p.add_argument("--mass-fraction", type=float, default=1e-6)
     p.add_argument("--nlambda", type=int, default=50)
@@ -376,9 +378,18 @@ def main():
     red = [torch.zeros(n, dtype=torch.float64, device="cuda") for n in sizes] if dist else None
     phases = ([A.PHASE_STELLAR] + [A.PHASE_DUST_SELFABS] * wl.selfabs_cycles +
               ([A.PHASE_DUST_EMISSION] if wl.dust_phase else []))
+    # launch choices (packets in flight, refill width, traversal blocks) from trial slices of the
+    # stellar phase: set-up, not timed
+    launch, tune_s = None, 0.0
+    if not args.no_autotune:
+        from skirt7_b200 import autotune
+        t0 = time.time()
+        launch = autotune.tune(ctx, A.PHASE_STELLAR, ells, Npp, precision=prec)
+        tune_s = time.time() - t0
 
     def run_phases(seed, stream):
-        ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=seed, precision=prec, stream=stream)
+        ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=seed, precision=prec, stream=stream,
+                      launch=launch)
         if wl.dust_phase:
             # PanMonteCarloSimulation::rundustselfabsorption / rundustemission (:106-187, :191-346):
             # before each dust phase the emission spectra follow from the absorbed luminosity
@@ -386,10 +397,10 @@ def main():
                 ctx.calc_dust_emission()
                 ctx.reset_dust_absorption()
                 ctx.run_phase(A.PHASE_DUST_SELFABS, ells, Npp, first, npp_rank, seed=seed + 2 + c, precision=prec,
-                              stream=stream)
+                              stream=stream, launch=launch)
             ctx.calc_dust_emission()            # PanDustSystem::calculatedustemission
             ctx.run_phase(A.PHASE_DUST_EMISSION, ells, Npp, first, npp_rank, seed=seed + 1, precision=prec,
-                          stream=stream)
+                          stream=stream, launch=launch)
 
     def step(seed):
         run_phases(seed, handle)
@@ -440,7 +451,7 @@ def main():
     # the dominant kernel; its device time is summed over the waves of the phase (CUDA events
     # around each launch on the launching stream)
     ctx.reset_tallies()
-    ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=999, precision=prec, stream=handle)
+    ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=999, precision=prec, stream=handle, launch=launch)
     ctx.sync()
     kms = ctx.last_phase_ms()
     ev_ms, trav_ms, waves = ctx.phase_times()
@@ -496,7 +507,9 @@ def main():
             "ms_per_step": total_ms / args.steps, "ms_steps": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if prec == A.PREC_FP32 else "f64", "data": "synthetic",
             "config": _config(args, wl),
-            "setup": {"grid_build_s": wl.grid_s, "grid": "device"},
+            "setup": {"grid_build_s": wl.grid_s, "grid": "device", "autotune_s": tune_s,
+                      "launch": {k: launch[k] for k in ("pool", "refill", "blocks")} if launch else "library defaults",
+                      "autotune_trials": launch["trials"] if launch else None},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "traffic_basis": ("scaled, not measured in this run: ncu DRAM bytes per cell step of "

@@ -214,10 +214,13 @@ typedef struct skg_run_opts {
     int32_t max_steps;                      /* per traversal cell-step budget (0 = default 1<<20) */
     int32_t max_scatt;                      /* per packet scattering budget (0 = default 100000) */
     int32_t blocks;                         /* traversal blocks per wave (0 = auto: resident blocks x SMs) */
-    int32_t threads;                        /* reserved (0) */
+    int32_t refill;                         /* traversal lanes of a warp that wait for a job before the warp
+                                               takes new ones, 1..32 (0 = default 8; the autotuner's choice) */
     int32_t dedupe_peeloff;                 /* share one peel-off traversal among instruments that see
                                                the packet from the same direction (same tau; default 1) */
-    int32_t pool;                           /* packets in flight per wave (0 = default 2^21) */
+    int32_t pool;                           /* packets in flight per wave (0 = default: 2^21, or 2^23 for a
+                                               skg_run_phase of at least 2^26 packets on a Cartesian or tree
+                                               grid) */
 } skg_run_opts;
 
 /* Counters of one phase run (device side, exact). */

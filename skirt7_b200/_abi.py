@@ -103,7 +103,7 @@ class Scene(C.Structure):
 class RunOpts(C.Structure):
     _fields_ = [
         ("precision", C.c_int32), ("max_steps", C.c_int32), ("max_scatt", C.c_int32),
-        ("blocks", C.c_int32), ("threads", C.c_int32), ("dedupe_peeloff", C.c_int32), ("pool", C.c_int32),
+        ("blocks", C.c_int32), ("refill", C.c_int32), ("dedupe_peeloff", C.c_int32), ("pool", C.c_int32),
     ]
 
 

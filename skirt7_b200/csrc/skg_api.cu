@@ -320,11 +320,11 @@ struct Staging {
         if (!hdr || !this->items || !grids || !scenes || !ells || !work || !err || !counters)
             throw Failure{SKG_ERR_OOM, "device allocation failed"};
     }
-    RunParams params(int max_scatt) const {
+    RunParams params(int max_scatt, int refill = 0) const {
         RunParams P;
         std::memset(&P, 0, sizeof(P));
         P.hdr = hdr; P.items = items; P.grids = grids; P.scenes = scenes; P.ells = ells;
-        P.max_scatt = max_scatt; P.work = work; P.err = err; P.counters = counters;
+        P.max_scatt = max_scatt; P.refill = refill; P.work = work; P.err = err; P.counters = counters;
         return P;
     }
 };
@@ -793,7 +793,11 @@ int skg_run_phase(skg_ctx* ctx, int phase, const int32_t* ells, int nell, uint64
         cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
         if (count == 0) return SKG_OK;
         const uint64_t total = (uint64_t)nell * count;
-        const size_t pool_max = (opts && opts->pool > 0) ? (size_t)opts->pool : ((size_t)1 << 21);
+        // packets in flight: 2^21 records (256 MB) by default; a large phase on a grid without
+        // re-walk checkpoints (1 KB per record on the Voronoi grid) takes 2^23 (1 GB of records,
+        // 4x fewer waves: the 5*10^8-packet octree phase 7.85 s against 8.14 s)
+        const bool big = total >= ((uint64_t)1 << 26) && ctx->grid.type != SKG_GRID_VORONOI;
+        const size_t pool_max = (opts && opts->pool > 0) ? (size_t)opts->pool : ((size_t)1 << (big ? 23 : 21));
         const size_t npool = (size_t)std::min<uint64_t>(total, pool_max);
         CK(ctx->waves.reserve(npool, ctx->hs.ngroups, ctx->grid.type));
         // one slot, one work item (pageable host sources: the copies are staged before return)
@@ -813,7 +817,8 @@ int skg_run_phase(skg_ctx* ctx, int phase, const int32_t* ells, int nell, uint64
         CK(cudaMemcpyAsync(T.ells, ells, nell * sizeof(int), cudaMemcpyHostToDevice, s));
         CK(cudaMemsetAsync(T.work, 0, sizeof(unsigned long long), s));
         CK(cudaMemsetAsync(T.err, 0, sizeof(unsigned), s));
-        RunParams P = T.params((opts && opts->max_scatt > 0) ? opts->max_scatt : 100000);
+        REQUIRE(!opts || (opts->refill >= 0 && opts->refill <= 32), "refill lanes must be in 0..32");
+        RunParams P = T.params((opts && opts->max_scatt > 0) ? opts->max_scatt : 100000, opts ? opts->refill : 0);
         int precision = opts ? opts->precision : SKG_PREC_FP32;
         int blocks = opts ? opts->blocks : 0;
         CK(cudaEventRecord(ctx->ev0, s));
@@ -905,15 +910,22 @@ int skg_read_absorption(skg_ctx* ctx, double* labs_stellar, double* labs_dust) {
     int rc = skg_sync(ctx, -1);
     if (rc) return rc;
     try {
-        size_t n = (size_t)ctx->ncells * ctx->nlambda;
-        if (labs_stellar) {
-            if (ctx->hs.labs_stel) CK(cudaMemcpy(labs_stellar, ctx->hs.labs_stel, n * sizeof(double), cudaMemcpyDeviceToHost));
-            else std::memset(labs_stellar, 0, n * sizeof(double));
-        }
-        if (labs_dust) {
-            if (ctx->hs.labs_dust) CK(cudaMemcpy(labs_dust, ctx->hs.labs_dust, n * sizeof(double), cudaMemcpyDeviceToHost));
-            else std::memset(labs_dust, 0, n * sizeof(double));
-        }
+        const size_t nc = (size_t)ctx->ncells, nl = (size_t)ctx->nlambda, n = nc * nl;
+        // the device tables are wavelength-major ([ell][m]); the caller gets [m][ell]
+        std::vector<double> t;
+        auto read = [&](const double* dev, double* out) {
+            if (!out) return;
+            if (!dev) { std::memset(out, 0, n * sizeof(double)); return; }
+            t.resize(n);
+            CK(cudaMemcpy(t.data(), dev, n * sizeof(double), cudaMemcpyDeviceToHost));
+            const size_t B = 64;                        // cache blocks of the transpose
+            for (size_t m0 = 0; m0 < nc; m0 += B)
+                for (size_t e0 = 0; e0 < nl; e0 += B)
+                    for (size_t m = m0; m < std::min(nc, m0 + B); m++)
+                        for (size_t e = e0; e < std::min(nl, e0 + B); e++) out[m * nl + e] = t[e * nc + m];
+        };
+        read(ctx->hs.labs_stel, labs_stellar);
+        read(ctx->hs.labs_dust, labs_dust);
         return SKG_OK;
     } catch (const Failure& f) { return fail(ctx, f); }
 }
@@ -1263,7 +1275,8 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
         for (skg_ctx* c : slots) ngroups = std::max(ngroups, c->hs.ngroups);
         if (total == 0) return SKG_OK;
         CK(b->waves.reserve(npool, ngroups, gtype));
-        RunParams P = b->T.params((opts && opts->max_scatt > 0) ? opts->max_scatt : 100000);
+        REQUIRE(!opts || (opts->refill >= 0 && opts->refill <= 32), "refill lanes must be in 0..32");
+        RunParams P = b->T.params((opts && opts->max_scatt > 0) ? opts->max_scatt : 100000, opts ? opts->refill : 0);
         Staging& T = b->T;
         auto enqueue = [&](cudaStream_t q) {
             CK(cudaMemcpyAsync(T.hdr, b->h_hdr, sizeof(BatchHeader), cudaMemcpyHostToDevice, q));

@@ -70,7 +70,7 @@ struct DevScene {
     int min_scatt_events;
     double xi;
     int store_abs;
-    double* labs_stel;        // [m*nl + ell]
+    double* labs_stel;        // [ell*ncells + m] (wavelength-major on the device)
     double* labs_dust;
 
     // dust emission sources
@@ -111,6 +111,7 @@ struct RunParams {
     const DevScene* const* scenes; // [nslots]
     const int* ells;
     int max_scatt;
+    int refill;                   // lanes of a warp that wait for a job before it takes new ones (0: default)
     unsigned long long* work;     // packet work counter
     unsigned int* err;            // error word
     unsigned long long* counters; // skg_counters layout

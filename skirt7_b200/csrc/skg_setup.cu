@@ -112,7 +112,7 @@ __global__ void dust_emission_kernel(const DevGrid g, const DevScene* __restrict
     double fac = 4.0 * M_PI * cell_volume(g, m);
     double rho = S.rho[m];
     for (int ell = 0; ell < nl; ell++) {
-        double la = S.labs_stel[(size_t)m * nl + ell] + S.labs_dust[(size_t)m * nl + ell];
+        double la = S.labs_stel[(size_t)ell * S.ncells + m] + S.labs_dust[(size_t)ell * S.ncells + m];
         lb += la;
         double kabs = S.kext[ell] * (1.0 - S.albedo[ell]);
         double J = la / (kabs * rho * fac) / S.dlambda[ell];
@@ -124,13 +124,13 @@ __global__ void dust_emission_kernel(const DevGrid g, const DevScene* __restrict
     double T = Tv[p] + ((pa - planckabs[p]) / (planckabs[p + 1] - planckabs[p])) * (Tv[p + 1] - Tv[p]);
     if (temperature) temperature[m] = T;
     double total = 0;
-    double* Lv = spectra + (size_t)m * nl;
+    const size_t nc = (size_t)S.ncells;
     for (int ell = 0; ell < nl; ell++) {
         double kabs = S.kext[ell] * (1.0 - S.albedo[ell]);
         double v = (T > 0) ? kabs * planck_B(S.lambda[ell], T) * S.dlambda[ell] : 0.0;
-        Lv[ell] = v; total += v;
+        spectra[ell * nc + m] = v; total += v;
     }
-    if (total > 0) for (int ell = 0; ell < nl; ell++) Lv[ell] /= total;
+    if (total > 0) for (int ell = 0; ell < nl; ell++) spectra[ell * nc + m] /= total;
 }
 
 cudaError_t launch_dust_emission(const DevGrid& g, const DevScene* dS, const double* Tv, const double* planckabs,
@@ -142,14 +142,14 @@ cudaError_t launch_dust_emission(const DevGrid& g, const DevScene* dS, const dou
     return cudaGetLastError();
 }
 
-// emit_Lv[ell][m] = Labsbol[m] * spectrum[m][ell]   (PanMonteCarloSimulation.cpp:197-203)
+// emit_Lv[ell][m] = Labsbol[m] * spectrum[ell][m]   (PanMonteCarloSimulation.cpp:197-203)
 __global__ void emission_weights_kernel(int nl, int nc, const double* __restrict__ labsbol,
                                         const double* __restrict__ spectra, double* emit_Lv) {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (int64_t)nl * nc) return;
     int ell = (int)(t / nc), m = (int)(t - (int64_t)ell * nc);
     double lb = labsbol[m];
-    emit_Lv[t] = (lb > 0.0) ? lb * spectra[(size_t)m * nl + ell] : 0.0;
+    emit_Lv[t] = (lb > 0.0) ? lb * spectra[t] : 0.0;
 }
 // NR::cdf normalisation (NR.hpp:388-394): P_0 = 0, P_{i+1} = sum_{j<=i} p_j / sum p
 __global__ void cdf_totals_kernel(int nl, int nc, double* cdf, double* Ltot) {

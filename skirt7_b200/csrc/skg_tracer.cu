@@ -154,6 +154,26 @@ template<typename R> SKG_D double kappa_rho(const DevScene& S, int m, int ell) {
 #ifndef SKG_DETECT_INLINE
 #define SKG_DETECT_INLINE 1
 #endif
+// frame pixel tallies: lanes of a warp that add to the same pixel sum their values over the warp
+// first and one of them adds (1), or every lane adds its own value (0)
+#ifndef SKG_WARP_AGG
+#define SKG_WARP_AGG 1
+#endif
+SKG_D void frame_add(double* addr, double v) {
+#if SKG_WARP_AGG
+    const unsigned act = __activemask();
+    const unsigned peers = __match_any_sync(act, (unsigned long long)addr);
+    if (peers & (peers - 1)) {
+        double s = 0;
+        for (unsigned m = peers; m; m &= m - 1) s += __shfl_sync(peers, v, __ffs(m) - 1);
+        v = s;
+    }
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(addr, v);
+#else
+    atomicAdd(addr, v);
+#endif
+}
+
 #if SKG_DETECT_INLINE
 __device__ __forceinline__
 #else
@@ -177,9 +197,9 @@ int detect_group(const DevScene& S, int grp, int ell, double Lpeel, double tau,
         size_t fp = (size_t)I.nxp * I.nyp;
         if (I.type == SKG_INSTR_FRAME) {
             if (l >= 0) {
-                atomicAdd(I.cube + (size_t)ell * fp + l, Lextf); adds++;
+                frame_add(I.cube + (size_t)ell * fp + l, Lextf); adds++;
                 // the frame of the packet's stellar component (component 1 + comp)
-                if (I.ncomp > 1 && comp >= 0) { atomicAdd(I.cube + ((size_t)(1 + comp) * nl + ell) * fp + l, Lextf); adds++; }
+                if (I.ncomp > 1 && comp >= 0) { frame_add(I.cube + ((size_t)(1 + comp) * nl + ell) * fp + l, Lextf); adds++; }
             }
         } else if (I.type == SKG_INSTR_SED) {
             sed_add(0, Lextf);
@@ -665,7 +685,9 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS) launch_kernel(const WavePar
 // traversal pass
 
 // Absorption in cell m of a path step: simulateescapeandabsorption (MonteCarloSimulation.cpp:441-462)
-// with OligoDustSystem::absorb / PanDustSystem::absorb.  v1 = L e^-tau on entry (a running product,
+// with OligoDustSystem::absorb / PanDustSystem::absorb.  The tables are wavelength-major on the
+// device ([ell][m]): a wave carries the packets of one or two wavelengths (packets are handed out
+// wavelength by wavelength), so its tallies fall in one slice of the table that stays in L2.  v1 = L e^-tau on entry (a running product,
 // one expm1 per absorbing step: L e^-tau (1 - e^-dtau) = -v1 expm1(-dtau)); v2 accumulates L_sca with
 // the local albedo when there are several dust components.  Returns 1 when a tally was stored.
 template<typename R>
@@ -678,7 +700,7 @@ SKG_D int absorb_step(const DevScene& S, int phase, int m, int ell, double dtau,
         const double em = expm1(-dtau);
         const double Lintm = -v1 * em;
         v1 += v1 * em;
-        atomicAdd(labs + (size_t)m * S.nlambda + ell, (1.0 - S.albedo[ell]) * Lintm);
+        atomicAdd(labs + (size_t)ell * S.ncells + m, (1.0 - S.albedo[ell]) * Lintm);
         return 1;
     }
     double ksca = 0, kext = 0;
@@ -692,7 +714,7 @@ SKG_D int absorb_step(const DevScene& S, int phase, int m, int ell, double dtau,
     v1 += v1 * em;
     v2 += alb * Lintm;
     if (!store) return 0;
-    atomicAdd(labs + (size_t)m * S.nlambda + ell, (1.0 - alb) * Lintm);
+    atomicAdd(labs + (size_t)ell * S.ncells + m, (1.0 - alb) * Lintm);
     return 1;
 }
 
@@ -801,6 +823,7 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
     unsigned* const taken = W.jcount + (MODE == 2 ? 4 : 2);
     const int phase = H.phase;
     const int lane = threadIdx.x & 31;
+    const int refill_lanes = P.refill > 0 ? P.refill : (MODE == 2 ? SKG_REFILL_PEEL : SKG_REFILL_LANES);
 
     int j = -1;                       // the lane's job (-1: none)
     int p = 0, slot = 0, ell = 0;
@@ -850,7 +873,7 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
             }
             continue;
         }
-        if (want && (__popc(want) >= (MODE == 2 ? SKG_REFILL_PEEL : SKG_REFILL_LANES) || (live & ~want & ~pend) == 0)) {
+        if (want && (__popc(want) >= refill_lanes || (live & ~want & ~pend) == 0)) {
             const int leader = __ffs(want) - 1;
             unsigned base = 0;
             if (lane == leader) base = atomicAdd(taken, (unsigned)__popc(want));

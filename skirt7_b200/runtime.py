@@ -28,6 +28,7 @@ class Context:
     def __init__(self, model: SceneModel, device=0):
         self.lib = A.load()
         self.model = model
+        self.device = device
         self.scene, self._keep = model.lower()
         h = C.c_void_p()
         A.check(self.lib.skg_ctx_create(C.byref(self.scene), device, C.byref(h)))
@@ -94,10 +95,14 @@ class Context:
 
     # ---- the packet loop
     def run_phase(self, phase, ells, npp, first=0, count=None, seed=4357, precision=A.PREC_FP32,
-                  max_steps=0, max_scatt=0, blocks=0, pool=0, stream=None):
-        """skg_run_phase.  pool: packets in flight per wave (0 = the library's default)."""
+                  max_steps=0, max_scatt=0, blocks=0, pool=0, stream=None, refill=0, launch=None):
+        """skg_run_phase.  pool: packets in flight per wave, blocks: traversal blocks, refill: lanes
+        of a warp that wait before it takes new jobs (0 = the library's defaults); launch: a dict
+        with any of these (an autotuner result) that takes their place."""
+        if launch:
+            pool, blocks, refill = launch.get("pool", pool), launch.get("blocks", blocks), launch.get("refill", refill)
         ells = np.ascontiguousarray(ells, dtype=np.int32)
-        opts = A.RunOpts(precision, max_steps, max_scatt, blocks, 0, 1, pool)
+        opts = A.RunOpts(precision, max_steps, max_scatt, blocks, refill, 1, pool)
         count = npp if count is None else count
         self._ck(self.lib.skg_run_phase(self.h, phase, ells.ctypes.data_as(A.i32p), len(ells), int(npp), int(first),
                                         int(count), int(seed), C.byref(opts), stream))
@@ -192,7 +197,7 @@ class Batch:
         self.h = h
         self._keep = []
 
-    def run(self, phase, slices, precision=A.PREC_FP32, graph=False, stream=None, max_scatt=0, pool=0):
+    def run(self, phase, slices, precision=A.PREC_FP32, graph=False, stream=None, max_scatt=0, pool=0, refill=0):
         """slices: list of (Context, ells, npp, first, count, seed)."""
         n = len(slices)
         arr = (A.Work * max(n, 1))()
@@ -201,7 +206,7 @@ class Batch:
             e = np.ascontiguousarray(ells, dtype=np.int32)
             keep.append(e)
             arr[i] = A.Work(ctx.h.value, e.ctypes.data_as(A.i32p), len(e), int(npp), int(first), int(count), int(seed))
-        opts = A.RunOpts(precision, 0, max_scatt, 0, 0, 1, pool)
+        opts = A.RunOpts(precision, 0, max_scatt, 0, refill, 1, pool)
         A.check(self.lib.skg_batch_run(self.h, phase, arr, n, C.byref(opts), A.BATCH_GRAPH if graph else 0, stream))
         self._keep = keep
 
@@ -311,7 +316,12 @@ class MonteCarloSimulation:
     persistent device launch over all wavelengths."""
 
     def __init__(self, model: SceneModel, packages, seed=4357, precision=A.PREC_FP32, device=0,
-                 selfAbsorption=False, cycles=0, emissionBoost=1.0, nprocs=1, rank=0):
+                 selfAbsorption=False, cycles=0, emissionBoost=1.0, nprocs=1, rank=0, threads=1, autotune=False):
+        """threads: the host thread count the reference would run with (its -t option): it sets the
+        chunking, hence the packet count actually run, totalChunks * chunksize >= packages
+        (MonteCarloSimulation.cpp:68-114).  autotune: before the first phase, time trial slices of
+        the stellar phase for the launch choices of skirt7_b200.autotune (True, or the path of a
+        JSON cache) and run every phase with the fastest."""
         self.model = model
         self.packages = packages
         self.seed = seed
@@ -321,6 +331,9 @@ class MonteCarloSimulation:
         self.cycles = cycles
         self.emissionBoost = emissionBoost
         self.nprocs, self.rank = nprocs, rank
+        self.threads = max(1, int(threads))
+        self.autotune = autotune
+        self.launch = None
         self.ctx = None
         self.phase_ms = {}
 
@@ -328,6 +341,29 @@ class MonteCarloSimulation:
         if self.ctx is None:
             self.ctx = Context(self.model, self.device)
         return self
+
+    def tune(self):
+        """The launch choices for this simulation's phases (skirt7_b200.autotune.tune on a slice of
+        the stellar phase); a tree grid whose rope records walk faster is rebuilt with them."""
+        from . import autotune
+        ctx = self.ctx
+        _, _, npp = chunk_params(self.packages, self.threads, self.nprocs, ctx.nlambda)
+        path = self.autotune if isinstance(self.autotune, str) else None
+        self.launch = autotune.tune(ctx, A.PHASE_STELLAR, np.arange(ctx.nlambda), npp, precision=self.precision,
+                                    path=path, records=True)
+        if self.launch.get("records") == "rope":
+            import os
+            ctx.close()
+            old = os.environ.get("SKG_TREE_RECORDS")
+            os.environ["SKG_TREE_RECORDS"] = "rope"
+            try:
+                self.ctx = Context(self.model, self.device)
+            finally:
+                if old is None:
+                    os.environ.pop("SKG_TREE_RECORDS", None)
+                else:
+                    os.environ["SKG_TREE_RECORDS"] = old
+        return self.launch
 
     def _packet_range(self, npp):
         # disjoint packet ranges per rank (MonteCarloSimulation.cpp:98-104 distributes chunks)
@@ -337,9 +373,9 @@ class MonteCarloSimulation:
 
     def _run(self, phase, packages, seed):
         ctx = self.ctx
-        _, _, npp = chunk_params(packages, 1, 1, ctx.nlambda)
+        _, _, npp = chunk_params(packages, self.threads, self.nprocs, ctx.nlambda)
         first, count = self._packet_range(npp)
-        ctx.run_phase(phase, np.arange(ctx.nlambda), npp, first, count, seed, self.precision)
+        ctx.run_phase(phase, np.arange(ctx.nlambda), npp, first, count, seed, self.precision, launch=self.launch)
         ctx.sync()
         return ctx.last_phase_ms() if count else 0.0
 
@@ -377,6 +413,8 @@ class MonteCarloSimulation:
 
     def run(self):
         self.setup()
+        if self.autotune and self.launch is None:
+            self.tune()
         self.runstellaremission()
         if self.model.dustEmission and self.model.dustComps:
             if self.selfAbsorption:

@@ -417,15 +417,23 @@ class SkiSimulation:
         self.grid_spec = None
         return self
 
-    def simulation(self, device=0, precision=A.PREC_FP32):
+    def simulation(self, device=0, precision=A.PREC_FP32, threads=1, autotune=False):
         from . import runtime
         self.setup_grid(device)
         return runtime.MonteCarloSimulation(self.model, self.packages, seed=self.seed, precision=precision,
                                             device=device, selfAbsorption=self.selfAbsorption, cycles=self.cycles,
-                                            emissionBoost=self.emissionBoost)
+                                            emissionBoost=self.emissionBoost, threads=threads, autotune=autotune)
 
-    def run(self, device=0, precision=A.PREC_FP32):
-        return self.simulation(device, precision).run()
+    def emulate(self):
+        """The reference's emulation mode (-e, SkirtCommandLineHandler.cpp:270-284): one photon
+        package per wavelength and no dust self-absorption -- the simulation is set up in full (grid,
+        densities, tables on the device) and its phases run with a single packet."""
+        self.packages = 1
+        self.selfAbsorption = False
+        return self
+
+    def run(self, device=0, precision=A.PREC_FP32, threads=1, autotune=False):
+        return self.simulation(device, precision, threads, autotune).run()
 
 
 def _voronoi_sites(model, spec, seed):

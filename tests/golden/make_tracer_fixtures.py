@@ -32,7 +32,7 @@ SCENES = {
                        packets=[4.4e6, 1.2e6, 3.0e5], batches=20),
     "kdtree_point": dict(model=scenes.kdtree_point_model, spec=scenes.KDTREE, ells=scenes.KDTREE_ELLS,
                          packets=[3.0e6, 4.0e5, 4.0e5], batches=20),
-    "voronoi_clumpy": dict(model=scenes.voronoi_clumpy_model, spec=None, ells=[0], packets=[1.2e6], batches=20),
+    "voronoi_clumpy": dict(model=scenes.voronoi_clumpy_model, spec=None, ells=[0], packets=[4.8e6], batches=20),
 }
 
 

@@ -18,9 +18,9 @@ def test_pool_and_blocks_do_not_change_results():
     m.rho = cell_center_density(m)
     ctx = runtime.Context(m)
     frames = []
-    for pool, blocks in ((1 << 12, 148), (1 << 16, 296), (1 << 20, 0)):
+    for pool, blocks, refill in ((1 << 12, 148, 4), (1 << 16, 296, 16), (1 << 20, 0, 0), (1 << 18, 0, 32)):
         ctx.reset_tallies()
-        ctx.run_phase(A.PHASE_STELLAR, [0], 60000, 0, 60000, seed=5, pool=pool, blocks=blocks)
+        ctx.run_phase(A.PHASE_STELLAR, [0], 60000, 0, 60000, seed=5, pool=pool, blocks=blocks, refill=refill)
         ctx.sync()
         frames.append(ctx.read_instrument(0)[0].copy())
         ev, tr, waves = ctx.phase_times()
@@ -31,8 +31,11 @@ def test_pool_and_blocks_do_not_change_results():
     cube, sed = ctx.read_instrument(0)
     c2, s2 = ctx.read_instrument(0, out=(np.empty(cube.size), np.empty(sed.size)))
     assert np.array_equal(c2, cube) and np.array_equal(s2, sed)
-    res = autotune.tune(ctx, A.PHASE_STELLAR, [0], 60000, sample=20000, pools=[1 << 12, 1 << 14], blocks=[148, 296])
-    assert res["pool"] in (1 << 12, 1 << 14) and res["blocks"] in (148, 296) and len(res["trials"]) == 4
+    res = autotune.tune(ctx, A.PHASE_STELLAR, [0], 60000, sample=20000, pools=[1 << 12, 1 << 14], refills=(4, 8),
+                        blocks=[148, 296])
+    assert res["pool"] in (1 << 12, 1 << 14) and res["blocks"] in (148, 296) and res["refill"] in (4, 8)
+    assert len(res["trials"]) == 4                      # the start, then one coordinate at a time
+    assert res["ms"] == min(t["ms"] for t in res["trials"])
     assert autotune.tune(ctx, A.PHASE_STELLAR, [0], 60000) is res          # cached per workload class
     ctx.close()
 

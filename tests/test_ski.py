@@ -117,3 +117,22 @@ def test_multiframe_instrument_for_fitskirt():
     bad = multi.replace("</frames>", other + "</frames>")
     with pytest.raises(ski.SkiError, match="different sizes"):
         ski.load(xml[:i0] + bad + xml[i1:])
+
+
+def test_command_line_ski_lookup_and_refused_options(tmp_path, capsys):
+    """SkirtCommandLineHandler::skifilesFor (SkirtCommandLineHandler.cpp:191-254): a missing .ski
+    extension is added; wildcards match in the file's directory, -r also in its subdirectories,
+    sorted by name ignoring case; -l and -x are refused as in a reference build without them."""
+    from skirt7_b200.__main__ import main, skifiles_for
+    (tmp_path / "sub").mkdir()
+    for f in ("b.ski", "A.ski", "c.txt", "sub/d.ski"):
+        (tmp_path / f).write_text("<skirt-simulation-hierarchy/>")
+    assert skifiles_for(str(tmp_path / "b"), False) == [str(tmp_path / "b.ski")]
+    assert skifiles_for(str(tmp_path / "nope"), False) == []
+    assert skifiles_for(str(tmp_path / "*.ski"), False) == [str(tmp_path / "A.ski"), str(tmp_path / "b.ski")]
+    assert skifiles_for(str(tmp_path / "*.ski"), True) == [str(tmp_path / "A.ski"), str(tmp_path / "b.ski"),
+                                                            str(tmp_path / "sub" / "d.ski")]
+    assert main(["-l", "1", str(tmp_path / "b.ski")]) == 1
+    assert main(["-x"]) == 1
+    assert main([str(tmp_path / "nope.ski")]) == 1
+    assert "does not exist" in capsys.readouterr().err

@@ -41,3 +41,29 @@ def test_ski_octree_builds_on_the_device():
     cube, _ = sim.ctx.read_instrument(0)
     assert cube.sum() > 0 and sim.ctx.counters()["errors"] == 0
     sim.ctx.close()
+
+
+def test_command_line_modes(tmp_path, capsys):
+    """The skirt command's modes (SkirtCommandLineHandler.cpp): -e sets the simulation up and runs
+    one package per wavelength; -t sets the chunking, so the packets run are the reference's
+    totalChunks * chunksize for that thread count; -k with -o writes next to the ski file; --autotune
+    picks launch choices before the first phase (results do not depend on them)."""
+    from skirt7_b200.__main__ import main
+    xml = open(CFG1).read().replace('packages="1e6"', 'packages="12345"')
+    xml = xml.replace('<LinMesh numBins="100"/>', '<LinMesh numBins="20"/>').replace(
+        '<LinMesh numBins="50"/>', '<LinMesh numBins="10"/>')
+    d = tmp_path / "runs"
+    d.mkdir()
+    f = d / "disk.ski"
+    f.write_text(xml)
+    assert main(["-e", str(f)]) == 0
+    out = capsys.readouterr().out
+    assert "emulation" in out and "device memory" in out
+    assert main(["-k", "-o", "out", "-t", "4", str(f)]) == 0
+    assert (d / "out").is_dir() and any(p.name.startswith("disk_") for p in (d / "out").iterdir())
+    # -t 4: 40 chunks of 309 packets (MonteCarloSimulation.cpp:86-94)
+    s = ski.load(str(f))
+    sim = s.run(threads=4, autotune=True)
+    assert sim.ctx.counters()["packets"] == 40 * 309
+    assert set(sim.launch) >= {"pool", "refill", "blocks"}
+    sim.ctx.close()
