@@ -67,8 +67,9 @@ def tune(ctx, phase, ells, npp, seed=777, precision=A.PREC_FP32, sample=None, po
 
     best_ms = run(best)
     for name, values in (("pool", pools), ("refill", refills), ("blocks", blocks)):
+        start = best[name]                       # timed already (with the other coordinates as now)
         for v in values:
-            if v == best[name]:
+            if v == start:
                 continue
             cand = dict(best, **{name: v})
             ms = run(cand)

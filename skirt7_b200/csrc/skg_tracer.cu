@@ -155,9 +155,12 @@ template<typename R> SKG_D double kappa_rho(const DevScene& S, int m, int ell) {
 #define SKG_DETECT_INLINE 1
 #endif
 // frame pixel tallies: lanes of a warp that add to the same pixel sum their values over the warp
-// first and one of them adds (1), or every lane adds its own value (0)
+// first and one of them adds (1), or every lane adds its own value (0).  Octree disk, 5*10^8
+// packets: phase 7870 ms with the aggregation against 7850-7930 ms without, event pass 652 against
+// 632-640 ms -- lanes of a warp rarely hit one pixel (their packets sit anywhere in the galaxy),
+// so the match costs more than the atomics it saves; off by default.
 #ifndef SKG_WARP_AGG
-#define SKG_WARP_AGG 1
+#define SKG_WARP_AGG 0
 #endif
 SKG_D void frame_add(double* addr, double v) {
 #if SKG_WARP_AGG
