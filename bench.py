@@ -63,6 +63,8 @@ def parse():
                    help="cache of the headline octree between runs of the same size (git-ignored)")
     p.add_argument("--serving", type=int, default=256,
                    help="requests of the fit-variant serving leg (Poisson 20/s; 0 = skip)")
+    p.add_argument("--serving-impl", default="native", choices=["native", "python"],
+                   help="the serving loop: the C ABI server (skg_submit/skg_poll) or the Python one")
     return p.parse_args()
 
 
@@ -553,20 +555,24 @@ def serving_leg(args, device):
     import numpy as np
     from skirt7_b200 import serving
     reqs = serving.fitskirt_requests(n=args.serving, rate=20.0, seed=2024)
-    srv = serving.Server(device=device, max_slots=64, npix=256)
     t0 = time.perf_counter()
-    done = srv.serve(reqs, realtime=True)
+    if args.serving_impl == "native":
+        done, nst = serving.serve_native(reqs, device=device, npix=256, max_slots=64)
+        ticks, tick_s, admit_s, peak = nst["ticks"], nst["tick_device_s"], None, None
+    else:
+        srv = serving.Server(device=device, max_slots=64, npix=256)
+        done = srv.serve(reqs, realtime=True)
+        srv.close()
+        ticks, tick_s, admit_s, peak = srv.ticks, srv.tick_gpu_s, srv.admit_s, srv.peak_resident
     wall = time.perf_counter() - t0
-    srv.close()
     st = serving.latency_stats(done)
     alone = sorted(serving.run_alone(r, device=device, npix=256)[1] for r in reqs)
     a50, a99 = float(np.percentile(alone, 50)), float(np.percentile(alone, 99))
     packets = sum(3 * r.packets for r in reqs)
-    return {"requests": len(reqs), "arrival_rate_per_s": 20.0, "p50_s": st["p50_s"], "p99_s": st["p99_s"],
-            "alone_p50_s": a50, "alone_p99_s": a99, "p99_over_alone_p99": st["p99_s"] / a99,
-            "packets_per_s": packets / wall, "makespan_s": wall, "ticks": srv.ticks,
-            "tick_device_s": srv.tick_gpu_s, "admit_host_s": srv.admit_s,
-            "peak_resident": srv.peak_resident}
+    return {"impl": args.serving_impl, "requests": len(reqs), "arrival_rate_per_s": 20.0, "p50_s": st["p50_s"],
+            "p99_s": st["p99_s"], "alone_p50_s": a50, "alone_p99_s": a99, "p99_over_alone_p99": st["p99_s"] / a99,
+            "packets_per_s": packets / wall, "makespan_s": wall, "ticks": ticks,
+            "tick_device_s": tick_s, "admit_host_s": admit_s, "peak_resident": peak}
 
 
 def cpu_baseline(args, wl, ctx):

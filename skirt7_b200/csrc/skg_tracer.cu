@@ -143,7 +143,21 @@ template<typename R> SKG_D double kappa_rho(const DevScene& S, int m, int ell) {
     return r;
 }
 
-// Instrument::detect for the members of one direction group after the shared traversal
+// kappa*rho of a cell step.  One dust component: kappa_ext of the job's wavelength is held by the
+// job (kext1 >= 0), and the FP32 walks multiply it in FP32 with the density embedded in the leaf
+// record (lattice tree walk) or the FP32 density table (Cartesian, Voronoi), without reading the
+// scene's tables every step; the FP64 walks keep the FP64 product of KappaRho.
+template<typename R>
+SKG_D double step_kr(const DevScene& S, float erho, float kext1, int m, int ell) {
+    if constexpr (sizeof(R) == 4) {
+        if (kext1 >= 0.f) return (double)(kext1 * (erho >= 0.f ? erho : __ldg(S.rhof + m)));
+        return kappa_rho<R>(S, m, ell);
+    } else {
+        return (kext1 >= 0.f && erho >= 0.f) ? (double)(kext1 * erho) : kappa_rho<R>(S, m, ell);
+    }
+}
+
+// Instrument::detect for the members of one direction group after the shared traversal// Instrument::detect for the members of one direction group after the shared traversal
 // (SEDInstrument.cpp:32-42, FrameInstrument.cpp:33-47, SimpleInstrument.cpp:35-49,
 // FullInstrument.cpp:109-177).  SED bins go to the block's private copy `psed` when it is given
 // (every packet of a wavelength adds to the same SED bin: global atomics would serialise on it).
@@ -917,7 +931,7 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
             if (st.walk(g, m, ds)) {
                 c_steps++;
                 // one dust component: the FP32 tree walk carries the cell density in its leaf record
-                const double kr = (kext1 >= 0.f && st.rho >= 0.f) ? (double)(kext1 * st.rho) : kappa_rho<R>(S, m, ell);
+                const double kr = step_kr<R>(S, st.rho, kext1, m, ell);
                 const double dtau = kr * (double)ds;
                 if (kind == 0) {
                     tau += dtau;
@@ -1002,7 +1016,7 @@ SKG_D double tail_tau(const DevGrid& g, const DevScene& S, int ell, R x, R y, R 
     int m; R ds;
     while (st.walk(g, m, ds)) {
         cnt[C_STEPS]++;
-        const double kr = (kext1 >= 0.f && st.rho >= 0.f) ? (double)(kext1 * st.rho) : kappa_rho<R>(S, m, ell);
+        const double kr = step_kr<R>(S, st.rho, kext1, m, ell);
         tau += kr * (double)ds;
     }
     cnt[C_TRAV]++; cnt[C_NBR] += st.nscanned(); cnt[C_FB] += st.fallbacks;
@@ -1049,7 +1063,7 @@ SKG_D void tail_path(const WaveParams& W, const DevGrid& g, const DevScene& S, i
     int m; R ds;
     while (st.walk(g, m, ds)) {
         cnt[C_STEPS]++;
-        const double kr = (kext1 >= 0.f && st.rho >= 0.f) ? (double)(kext1 * st.rho) : kappa_rho<R>(S, m, ell);
+        const double kr = step_kr<R>(S, st.rho, kext1, m, ell);
         const double dtau = kr * (double)ds;
         cnt[C_ABS] += absorb_step<R>(S, phase, m, ell, dtau, v1, v2);
         tau += dtau;
@@ -1078,7 +1092,7 @@ SKG_D void tail_path(const WaveParams& W, const DevGrid& g, const DevScene& S, i
     }
     while (st.walk(g, m, ds)) {
         cnt[C_STEPS]++;
-        const double kr = (kext1 >= 0.f && st.rho >= 0.f) ? (double)(kext1 * st.rho) : kappa_rho<R>(S, m, ell);
+        const double kr = step_kr<R>(S, st.rho, kext1, m, ell);
         const double tn = tau + kr * (double)ds, sn = s + (double)ds;
         if (tn > tau_int) {
             K.s_int = s + ((tau_int - tau) / (tn - tau)) * (sn - s);
