@@ -57,6 +57,15 @@ def ref():
         R.ref_lambertw1.restype = C.c_double
         R.ref_lambertw1.argtypes = [C.c_double]
         R.ref_sersic.argtypes = [C.c_double, dp, C.c_int, dp, dp, dp, C.c_int, dp]
+        if hasattr(R, "ref_cartesian_paths"):
+            R.ref_cartesian_paths.restype = C.c_int64
+            R.ref_cartesian_paths.argtypes = [dp, dp, C.c_int, dp, C.c_int, dp, C.c_int, dp, dp, C.c_int64, i32p, dp,
+                                              i64p, C.c_int64]
+            R.ref_tree_paths.restype = C.c_int64
+            R.ref_tree_paths.argtypes = [C.c_int, dp, C.POINTER(C.c_uint8), C.c_int64, C.c_int, dp, dp, C.c_int64,
+                                         i32p, dp, i64p, C.c_int64]
+            R.ref_voronoi_paths.restype = C.c_int64
+            R.ref_voronoi_paths.argtypes = [dp, C.c_int, dp, dp, dp, C.c_int64, i32p, dp, i64p, C.c_int64]
         _ref = R
     return _ref
 
@@ -323,3 +332,49 @@ def voronoi_mesh(sites, extent):
     boff = np.zeros(nb ** 3 + 1, dtype=np.int64)
     boff[1:] = np.cumsum(np.bincount(block, minlength=nb ** 3))
     return VoronoiDustGrid(EXT, s, off, ids, nb, boff, cell[order].astype(np.int32), vol, bb)
+
+
+def _ref_trace(call, r, k):
+    r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
+    k = np.ascontiguousarray(k, dtype=np.float64).reshape(-1, 3)
+    n = len(r)
+    off = np.zeros(n + 1, dtype=np.int64)
+    cap = 64 * max(n, 1)
+    while True:
+        cells, ds = np.zeros(cap, dtype=np.int32), np.zeros(cap)
+        tot = call(r.ctypes.data_as(dp), k.ctypes.data_as(dp), n, cells.ctypes.data_as(i32p), ds.ctypes.data_as(dp),
+                   off.ctypes.data_as(i64p), cap)
+        if tot <= cap:
+            return off, cells[:tot], ds[:tot]
+        cap = int(tot)
+
+
+def ref_cartesian_paths(grid, r, k):
+    """CartesianDustGrid::path of the reference itself (compiled in oracle/_ref) on a grid's planes."""
+    R = ref()
+    ext = np.ascontiguousarray([grid.minX, grid.minY, grid.minZ, grid.maxX, grid.maxY, grid.maxZ], dtype=np.float64)
+    xv, yv, zv = (np.ascontiguousarray(v, dtype=np.float64) for v in (grid.xv, grid.yv, grid.zv))
+    return _ref_trace(lambda rp, kp, n, c, d, o, cap: R.ref_cartesian_paths(
+        ext.ctypes.data_as(dp), xv.ctypes.data_as(dp), len(xv) - 1, yv.ctypes.data_as(dp), len(yv) - 1,
+        zv.ctypes.data_as(dp), len(zv) - 1, rp, kp, n, c, d, o, cap), r, k)
+
+
+def ref_voronoi_paths(sites, extent, r, k):
+    """VoronoiMesh::path of the reference itself on the mesh it builds from the sites (Voro++,
+    its block lists and kd-trees)."""
+    R = ref()
+    s = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+    ext = np.ascontiguousarray(extent, dtype=np.float64)
+    return _ref_trace(lambda rp, kp, n, c, d, o, cap: R.ref_voronoi_paths(
+        s.ctypes.data_as(dp), len(s), ext.ctypes.data_as(dp), rp, kp, n, c, d, o, cap), r, k)
+
+
+def ref_tree_paths(gtype, extent, split, search, r, k):
+    """TreeDustGrid::path of the reference itself (compiled in oracle/_ref) on the octree
+    (gtype 1) or k-d tree (2) that its node classes build from the split decisions."""
+    R = ref()
+    ext = np.ascontiguousarray(extent, dtype=np.float64)
+    sp = np.ascontiguousarray(split, dtype=np.uint8)
+    return _ref_trace(lambda rp, kp, n, c, d, o, cap: R.ref_tree_paths(
+        int(gtype), ext.ctypes.data_as(dp), sp.ctypes.data_as(C.POINTER(C.c_uint8)), len(sp), int(search), rp, kp, n,
+        c, d, o, cap), r, k)
