@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--workload", default="octree_pan", choices=WORKLOADS)
     p.add_argument("--packets", type=float, default=1e7, help="packets per wavelength per GPU per step")
     p.add_argument("--e2e-steps", type=int, default=5, help="steps of the end-to-end leg (at most --steps)")
+    p.add_argument("--plain-packets", type=float, default=1e6,
+                   help="packets per wavelength of the plain-GPU leg (one thread per packet; 0 = skip)")
     p.add_argument("--no-autotune", action="store_true",
                    help="run with the library's default launch choices instead of the autotuner's (set-up, untimed)")
     p.add_argument("--max-level", type=int, default=10)
@@ -495,6 +497,24 @@ def main():
         e2e_s = float(t.item())
     e2e = Npp * nl * len(phases) * e2e_steps / e2e_s
 
+    # the plain GPU path of the same device code: one thread per packet runs its whole life (the
+    # tail pass takes the phase over after its first wave: no wavefront, no job lists), on a
+    # sample of the workload's packets
+    plain = None
+    if rank == 0 and world == 1 and args.plain_packets > 0:
+        npl = int(args.plain_packets)
+        os.environ["SKG_TAIL_DIV"] = "1"
+        try:
+            ctx.reset_tallies()
+            ctx.run_phase(A.PHASE_STELLAR, ells, npl, 0, npl, seed=777, precision=prec, stream=handle)
+            ctx.sync()
+            pms = ctx.last_phase_ms()
+        finally:
+            del os.environ["SKG_TAIL_DIV"]
+        plain = {"value": npl * nl / (pms / 1e3), "unit": "packets/s", "packets": npl * nl, "phase_ms": pms,
+                 "how": "the stellar phase with one thread per packet for its whole life (the same device "
+                        "functions in one persistent kernel after the first wave: no wavefront passes)"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, wl, ctx)
@@ -530,6 +550,8 @@ def main():
             "clocks": clk,
             "counters_stellar_phase": c,
         }
+        if plain:
+            line["plain_gpu"] = plain
         if cpu:
             line["cpu_baseline"] = cpu
         if srv:
@@ -551,7 +573,8 @@ def serving_leg(args, device):
     """Fit-variant requests (oligochromatic disk, 3 wavelengths, Cartesian N^3 with N in 32..128,
     packets per wavelength log-uniform in 1e5..1e7, one 256x256 frame) arriving as a Poisson stream
     at 20/s, served by continuous batching; then every request alone on the idle device (the plain
-    single-simulation path).  Latency = result in host memory minus arrival."""
+    single-simulation path), and the plain path serving the same stream one request at a time.
+    Latency = result in host memory minus arrival."""
     import numpy as np
     from skirt7_b200 import serving
     reqs = serving.fitskirt_requests(n=args.serving, rate=20.0, seed=2024)
@@ -566,11 +589,21 @@ def serving_leg(args, device):
         ticks, tick_s, admit_s, peak = srv.ticks, srv.tick_gpu_s, srv.admit_s, srv.peak_resident
     wall = time.perf_counter() - t0
     st = serving.latency_stats(done)
-    alone = sorted(serving.run_alone(r, device=device, npix=256)[1] for r in reqs)
+    service = [serving.run_alone(r, device=device, npix=256)[1] for r in reqs]
+    alone = sorted(service)
     a50, a99 = float(np.percentile(alone, 50)), float(np.percentile(alone, 99))
+    # the plain single-simulation path serving the same stream: one request at a time in arrival
+    # order, each taking its measured alone time (start = max(arrival, previous finish))
+    finish, plain = 0.0, []
+    for r, t in sorted(zip(reqs, service), key=lambda q: q[0].arrival):
+        finish = max(r.arrival, finish) + t
+        plain.append(finish - r.arrival)
+    f99 = float(np.percentile(plain, 99))
     packets = sum(3 * r.packets for r in reqs)
     return {"impl": args.serving_impl, "requests": len(reqs), "arrival_rate_per_s": 20.0, "p50_s": st["p50_s"],
             "p99_s": st["p99_s"], "alone_p50_s": a50, "alone_p99_s": a99, "p99_over_alone_p99": st["p99_s"] / a99,
+            "plain_fifo_p50_s": float(np.percentile(plain, 50)), "plain_fifo_p99_s": f99,
+            "p99_over_plain_fifo_p99": st["p99_s"] / f99,
             "packets_per_s": packets / wall, "makespan_s": wall, "ticks": ticks,
             "tick_device_s": tick_s, "admit_host_s": admit_s, "peak_resident": peak}
 

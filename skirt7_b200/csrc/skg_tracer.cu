@@ -33,6 +33,7 @@
 #include "skg_scene.cuh"
 #include "skg_internal.h"
 #include "skg_wave.h"
+#include <type_traits>
 
 #include <chrono>
 #include <cstdlib>
@@ -143,17 +144,25 @@ template<typename R> SKG_D double kappa_rho(const DevScene& S, int m, int ell) {
     return r;
 }
 
+// Does the stepper carry the density of the step's cell in its leaf record (a data member rho),
+// or not (a static constant rho = -1)?
+template<typename St> struct EmbeddedRho {
+    static constexpr bool value = !std::is_same<decltype(&St::rho), const float*>::value;
+};
+
 // kappa*rho of a cell step.  One dust component: kappa_ext of the job's wavelength is held by the
-// job (kext1 >= 0), and the FP32 walks multiply it in FP32 with the density embedded in the leaf
-// record (lattice tree walk) or the FP32 density table (Cartesian, Voronoi), without reading the
-// scene's tables every step; the FP64 walks keep the FP64 product of KappaRho.
-template<typename R>
-SKG_D double step_kr(const DevScene& S, float erho, float kext1, int m, int ell) {
-    if constexpr (sizeof(R) == 4) {
-        if (kext1 >= 0.f) return (double)(kext1 * (erho >= 0.f ? erho : __ldg(S.rhof + m)));
+// job (kext1 >= 0) and multiplied in FP32 with the density embedded in the leaf record (tree
+// walks), or, in the FP32 walks without records (Cartesian, Voronoi), with the FP32 density table,
+// instead of reading the scene's tables every step; the FP64 walks keep the FP64 product of
+// KappaRho.  Resolved at compile time per stepper: a run-time choice between the two made the
+// lattice walk load the table every step as well (octree traversal pass 7819 against 7212 ms).
+template<typename R, typename St>
+SKG_D double step_kr(const DevScene& S, const St& st, float kext1, int m, int ell) {
+    if constexpr (sizeof(R) == 4 && !EmbeddedRho<St>::value) {
+        if (kext1 >= 0.f) return (double)(kext1 * __ldg(S.rhof + m));
         return kappa_rho<R>(S, m, ell);
     } else {
-        return (kext1 >= 0.f && erho >= 0.f) ? (double)(kext1 * erho) : kappa_rho<R>(S, m, ell);
+        return (kext1 >= 0.f && st.rho >= 0.f) ? (double)(kext1 * st.rho) : kappa_rho<R>(S, m, ell);
     }
 }
 
@@ -931,7 +940,7 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
             if (st.walk(g, m, ds)) {
                 c_steps++;
                 // one dust component: the FP32 tree walk carries the cell density in its leaf record
-                const double kr = step_kr<R>(S, st.rho, kext1, m, ell);
+                const double kr = step_kr<R>(S, st, kext1, m, ell);
                 const double dtau = kr * (double)ds;
                 if (kind == 0) {
                     tau += dtau;
@@ -1016,7 +1025,7 @@ SKG_D double tail_tau(const DevGrid& g, const DevScene& S, int ell, R x, R y, R 
     int m; R ds;
     while (st.walk(g, m, ds)) {
         cnt[C_STEPS]++;
-        const double kr = step_kr<R>(S, st.rho, kext1, m, ell);
+        const double kr = step_kr<R>(S, st, kext1, m, ell);
         tau += kr * (double)ds;
     }
     cnt[C_TRAV]++; cnt[C_NBR] += st.nscanned(); cnt[C_FB] += st.fallbacks;
@@ -1063,7 +1072,7 @@ SKG_D void tail_path(const WaveParams& W, const DevGrid& g, const DevScene& S, i
     int m; R ds;
     while (st.walk(g, m, ds)) {
         cnt[C_STEPS]++;
-        const double kr = step_kr<R>(S, st.rho, kext1, m, ell);
+        const double kr = step_kr<R>(S, st, kext1, m, ell);
         const double dtau = kr * (double)ds;
         cnt[C_ABS] += absorb_step<R>(S, phase, m, ell, dtau, v1, v2);
         tau += dtau;
@@ -1092,7 +1101,7 @@ SKG_D void tail_path(const WaveParams& W, const DevGrid& g, const DevScene& S, i
     }
     while (st.walk(g, m, ds)) {
         cnt[C_STEPS]++;
-        const double kr = step_kr<R>(S, st.rho, kext1, m, ell);
+        const double kr = step_kr<R>(S, st, kext1, m, ell);
         const double tn = tau + kr * (double)ds, sn = s + (double)ds;
         if (tn > tau_int) {
             K.s_int = s + ((tau_int - tau) / (tn - tau)) * (sn - s);
