@@ -67,6 +67,10 @@ def parse():
                    help="requests of the fit-variant serving leg (Poisson 20/s; 0 = skip)")
     p.add_argument("--serving-impl", default="native", choices=["native", "python"],
                    help="the serving loop: the C ABI server (skg_submit/skg_poll) or the Python one")
+    p.add_argument("--phase-only", action="store_true",
+                   help="run one stellar phase of the workload (--packets per wavelength, the library's default "
+                        "launch choices) and print its counters and pass times: the program the ncu captures "
+                        "of a phase run")
     return p.parse_args()
 
 
@@ -382,6 +386,14 @@ def main():
     red = [torch.zeros(n, dtype=torch.float64, device="cuda") for n in sizes] if dist else None
     phases = ([A.PHASE_STELLAR] + [A.PHASE_DUST_SELFABS] * wl.selfabs_cycles +
               ([A.PHASE_DUST_EMISSION] if wl.dust_phase else []))
+    if args.phase_only:
+        ctx.run_phase(A.PHASE_STELLAR, ells, Npp, first, npp_rank, seed=5, precision=prec)
+        ctx.sync()
+        ev_ms, trav_ms, waves = ctx.phase_times()
+        print(json.dumps({"workload": wl.name, "packets_per_wavelength": npp_rank, "counters": ctx.counters(),
+                          "event_pass_ms": ev_ms, "traversal_pass_ms": trav_ms, "waves": waves}))
+        ctx.close()
+        return
     # launch choices (packets in flight, refill width, traversal blocks) from trial slices of the
     # stellar phase: set-up, not timed
     launch, tune_s = None, 0.0
@@ -407,6 +419,10 @@ def main():
                           stream=stream, launch=launch)
 
     def step(seed):
+        # every step is a whole simulation from zero tallies: the dust phases' work depends on the
+        # absorbed luminosities, which must not pile up over the steps
+        ctx.reset_tallies()
+        ctx.sync()
         run_phases(seed, handle)
         # the phase is finished: the host has seen its last wave's counters and enqueued every wave,
         # so the step's end event follows all of them

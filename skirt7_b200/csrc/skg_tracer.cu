@@ -166,7 +166,7 @@ SKG_D double step_kr(const DevScene& S, const St& st, float kext1, int m, int el
     }
 }
 
-// Instrument::detect for the members of one direction group after the shared traversal// Instrument::detect for the members of one direction group after the shared traversal
+// Instrument::detect for the members of one direction group after the shared traversal
 // (SEDInstrument.cpp:32-42, FrameInstrument.cpp:33-47, SimpleInstrument.cpp:35-49,
 // FullInstrument.cpp:109-177).  SED bins go to the block's private copy `psed` when it is given
 // (every packet of a wavelength adds to the same SED bin: global atomics would serialise on it).
@@ -931,61 +931,72 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
 
         if (j < 0 || kind == 3) continue;   // waiting for enough lanes to refill / end paths together
 
-        // cell steps: up to SKG_INNER_STEPS of them before the warp looks at refills again
         const DevGrid& g = sg[slot];
         const DevScene& S = *s_scene[slot];
+        // one cell step of the job (m, ds, kappa*rho); true when it ended the job (a re-walk that
+        // reached the interaction optical depth)
+        auto take_step = [&](int m, R ds, double kr) -> bool {
+            c_steps++;
+            const double dtau = kr * (double)ds;
+            if (kind == 0) {
+                tau += dtau;
+            } else if (kind == 1) {
+                if (absorb_step<R>(S, phase, m, ell, dtau, v1, v2)) atomicAdd(&s_cnt[C_ABS], 1ull);
+                tau += dtau;
+                if constexpr (CKPT) {
+                    if (W.ckpt && nck < SKG_CKPT_N && st.steps >= (nck + 1) * SKG_CKPT_STRIDE && !st.done) {
+                        save_ckpt(W, p, nck, st, tau);
+                        nck++;
+                    }
+                }
+            } else {
+                const double tn = tau + dtau, sn = v1 + (double)ds;
+                if (tn > v2) {
+                    Packet& K = W.pk[p];
+                    K.s_int = v1 + ((v2 - tau) / (tn - tau)) * (sn - v1);
+                    K.int_cell = m;
+                    K.state = PK_INTERACT;
+                    atomicAdd(&s_cnt[C_TRAV], 1ull);
+                    atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.nscanned());
+                    atomicAdd(&s_cnt[C_FB], (unsigned long long)st.fallbacks);
+                    j = -1;
+                    return true;
+                }
+                tau = tn; v1 = sn;
+            }
+            return false;
+        };
+        // the traversal reached the edge of the grid
+        auto at_edge = [&]() {
+            atomicAdd(&s_cnt[C_TRAV], 1ull);
+            atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.nscanned());
+            atomicAdd(&s_cnt[C_FB], (unsigned long long)st.fallbacks);
+            if (st.steps > g.max_steps) { atomicOr(P.err, ERR_STEP_BUDGET); atomicAdd(&s_cnt[C_ERR], 1ull); }
+            if (kind == 0) {
+                W.jtau[j] = tau;
+                j = -1;
+            } else if (kind == 1) {
+                kind = 3;                       // the end of the path runs with other lanes' (above)
+            } else {
+                // DustGridPath::pathlength: an optical depth beyond the last segment gives the full length
+                Packet& K = W.pk[p];
+                K.s_int = v1; K.int_cell = -1; K.state = PK_INTERACT;
+                j = -1;
+            }
+        };
+
+        // cell steps: up to SKG_INNER_STEPS of them before the warp looks at refills again.  (Walking
+        // four steps ahead and loading their densities together, for the walks whose records do
+        // not carry the density, was slower: Cartesian traversal pass 83 against 64 ms, Voronoi
+        // peel-off walks 298 against 258 ms; the walk is issue-bound, not waiting on those loads.)
 #pragma unroll 1
         for (int is = 0; is < (MODE == 2 ? SKG_INNER_STEPS : SKG_INNER_PATH); is++) {
             int m; R ds;
             if (st.walk(g, m, ds)) {
-                c_steps++;
                 // one dust component: the FP32 tree walk carries the cell density in its leaf record
-                const double kr = step_kr<R>(S, st, kext1, m, ell);
-                const double dtau = kr * (double)ds;
-                if (kind == 0) {
-                    tau += dtau;
-                } else if (kind == 1) {
-                    if (absorb_step<R>(S, phase, m, ell, dtau, v1, v2)) atomicAdd(&s_cnt[C_ABS], 1ull);
-                    tau += dtau;
-                    if constexpr (CKPT) {
-                        if (W.ckpt && nck < SKG_CKPT_N && st.steps >= (nck + 1) * SKG_CKPT_STRIDE && !st.done) {
-                            save_ckpt(W, p, nck, st, tau);
-                            nck++;
-                        }
-                    }
-                } else {
-                    const double tn = tau + dtau, sn = v1 + (double)ds;
-                    if (tn > v2) {
-                        Packet& K = W.pk[p];
-                        K.s_int = v1 + ((v2 - tau) / (tn - tau)) * (sn - v1);
-                        K.int_cell = m;
-                        K.state = PK_INTERACT;
-                        atomicAdd(&s_cnt[C_TRAV], 1ull);
-                        atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.nscanned());
-                        atomicAdd(&s_cnt[C_FB], (unsigned long long)st.fallbacks);
-                        j = -1;
-                        break;
-                    } else {
-                        tau = tn; v1 = sn;
-                    }
-                }
+                if (take_step(m, ds, step_kr<R>(S, st, kext1, m, ell))) break;
             } else {
-                // the traversal reached the edge of the grid
-                atomicAdd(&s_cnt[C_TRAV], 1ull);
-                atomicAdd(&s_cnt[C_NBR], (unsigned long long)st.nscanned());
-                atomicAdd(&s_cnt[C_FB], (unsigned long long)st.fallbacks);
-                if (st.steps > g.max_steps) { atomicOr(P.err, ERR_STEP_BUDGET); atomicAdd(&s_cnt[C_ERR], 1ull); }
-                if (kind == 0) {
-                    W.jtau[j] = tau;
-                    j = -1;
-                } else if (kind == 1) {
-                    kind = 3;                       // the end of the path runs with other lanes' (above)
-                } else {
-                    // DustGridPath::pathlength: an optical depth beyond the last segment gives the full length
-                    Packet& K = W.pk[p];
-                    K.s_int = v1; K.int_cell = -1; K.state = PK_INTERACT;
-                    j = -1;
-                }
+                at_edge();
                 break;
             }
         }
