@@ -353,7 +353,11 @@ int  skg_batch_last_ms(skg_batch* b, float* ms);
    its own, and runs ticks -- one batched launch (skg_batch_run) carrying the next packet slice of
    every admitted request, oldest first up to tick_budget packets -- so that requests arriving
    while others run join the next tick.  A request retires when all its packets have run: its
-   instrument's tallies are copied into the caller's buffers and its context is freed.  Its
+   instrument's tallies are copied into the caller's buffers and its context is freed by a third
+   host thread, off the ticks' path.  skg_server_create raises the release threshold of the
+   device's default memory pool (cudaMemPoolAttrReleaseThreshold) to at least hbm_budget for the
+   process, so that freed context memory is kept for the next contexts instead of being unmapped
+   at each synchronisation (contexts allocate stream-ordered from that pool).  Its
    packets draw from streams keyed by its seed and packet index, so its result equals the same
    simulation run alone (skg_run_phase with count = npp) up to the order of the FP64 tally
    additions.  The stellar emission phase is served. */

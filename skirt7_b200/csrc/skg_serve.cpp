@@ -4,23 +4,35 @@
 // The caller is FitSKIRT's variant loop (FitSKIRTcore/OligoFitScheme.cpp:123-149 evaluates each
 // parameter set through AdjustableSkirtSimulation::performWith, AdjustableSkirtSimulation.cpp:
 // 145-194): many short simulations of one ski file with a few values substituted, each waiting for
-// its frames.  A server owns two host threads and works only through the public C ABI:
+// its frames.  A server owns three host threads and works through the public C ABI (and the
+// device's memory pool, below):
 //
-//   loop thread   admits submitted requests in arrival order while a batch slot is free and the
-//                 request's device-memory bound fits the budget (admission by HBM footprint);
-//                 runs ticks -- one skg_batch_run carrying the next packet slice of every
-//                 admitted request whose context is ready, oldest requests first up to a packet
-//                 budget per tick -- so that requests arriving meanwhile join a later tick and
-//                 their work overlaps on the device; retires a request once all its packets have
-//                 run: reads its tallies into the caller's buffers, frees its context, releases
-//                 its reservation;
-//   set-up thread builds the contexts of admitted requests (skg_ctx_create: uploads, density
-//                 sampling) while the ticks run.
+//   loop thread     admits submitted requests in arrival order while a batch slot is free and the
+//                   request's device-memory bound fits the budget (admission by HBM footprint);
+//                   runs ticks -- one skg_batch_run carrying the next packet slice of every
+//                   admitted request whose context is ready, oldest requests first up to a packet
+//                   budget per tick -- so that requests arriving meanwhile join a later tick and
+//                   their work overlaps on the device; retires a request once all its packets
+//                   have run: reads its tallies into the caller's buffers and hands its context
+//                   to the clean-up thread;
+//   set-up thread   builds the contexts of admitted requests (skg_ctx_create: uploads, density
+//                   sampling) while the ticks run;
+//   clean-up thread frees retired contexts, then releases their reservations: the next tick does
+//                   not wait for it.
+//
+// The device's default memory pool, from which contexts allocate (stream-ordered), keeps up to the
+// server's HBM budget of freed memory instead of returning it to the driver at each
+// synchronisation: a retired context's memory goes to the next one without being unmapped and
+// mapped again.  (Returned and mapped again, context set-up took 20-50 ms and release up to 0.75 s
+// on the fit-variant stream, and releases under the loop's lock left the device idle for 2.3 of
+// 17.6 s.)
 //
 // A request's packets draw from streams keyed by its seed and the packet index, so its result is
 // the same in whichever ticks it runs, alone or mixed with others, up to the summation order of
 // the FP64 tally atomics.
 #include "../../include/skirt_b200.h"
+
+#include <cuda_runtime.h>
 
 #include <algorithm>
 #include <chrono>
@@ -114,6 +126,7 @@ struct Req {
     double* cube = nullptr;
     double* sed = nullptr;
     int64_t footprint = 0;
+    int64_t held = 0;         // the reservation it holds (its footprint once admitted)
     ReqState state = QUEUED;
     skg_ctx* ctx = nullptr;
     uint64_t next = 0;        // first packet of the next slice
@@ -153,26 +166,45 @@ struct skg_server {
     std::deque<Req*> pending;            // submitted, not admitted (arrival order)
     std::deque<Req*> to_build;           // admitted, context not built yet
     std::vector<Req*> admitted;          // admitted, in arrival order
+    std::condition_variable free_cv;
+    std::deque<std::pair<skg_ctx*, int64_t>> to_free;   // retired contexts and their reservations
     int64_t next_id = 1, reserved = 0;
-    bool stop = false;
-    std::thread loop_thread, setup_thread;
+    bool stop = false, stop_free = false;
+    std::thread loop_thread, setup_thread, free_thread;
     // statistics
     int64_t ticks = 0, completed = 0, packets = 0;
     double tick_ms = 0;
 
     void setup_main();
     void loop_main();
+    void free_main();
     void finish(Req* r, int status, const std::string& msg);
 };
 
 void skg_server::finish(Req* r, int status, const std::string& msg) {
-    // caller holds mu
+    // caller holds mu; the context and the reservation go to the clean-up thread
     r->status = status; r->error = msg; r->state = DONE; r->done = Clock::now();
-    if (r->ctx) { skg_ctx_destroy(r->ctx); r->ctx = nullptr; }
-    reserved -= r->footprint;
+    to_free.emplace_back(r->ctx, r->held);
+    r->ctx = nullptr; r->held = 0;
     r->scene.reset();
     completed++;
     done_cv.notify_all();
+    free_cv.notify_one();
+}
+
+void skg_server::free_main() {
+    std::unique_lock<std::mutex> lk(mu);
+    while (true) {
+        free_cv.wait(lk, [&] { return stop_free || !to_free.empty(); });
+        if (to_free.empty()) return;             // stop_free and nothing left
+        auto [ctx, bytes] = to_free.front();
+        to_free.pop_front();
+        lk.unlock();
+        if (ctx) skg_ctx_destroy(ctx);
+        lk.lock();
+        reserved -= bytes;
+        cv.notify_all();                         // admission may proceed
+    }
 }
 
 void skg_server::setup_main() {
@@ -221,6 +253,7 @@ void skg_server::loop_main() {
             if (!admitted.empty() && reserved + r->footprint > opts.hbm_budget) break;
             pending.pop_front();
             reserved += r->footprint;
+            r->held = r->footprint;
             admitted.push_back(r);
             to_build.push_back(r);
             setup_cv.notify_one();
@@ -302,8 +335,18 @@ int skg_server_create(int device, const skg_server_opts* opts, skg_server** out)
         (s->opts.precision != SKG_PREC_FP32 && s->opts.precision != SKG_PREC_FP64)) { delete s; return SKG_ERR_INVALID; }
     const int rc = skg_batch_create(device, s->opts.max_slots, s->opts.max_slots, 64 * s->opts.max_slots, &s->batch);
     if (rc) { delete s; return rc; }
+    // freed context memory stays in the device's default pool up to the budget (see above)
+    cudaMemPool_t pool;
+    if (cudaSetDevice(device) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = 0;
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        keep = std::max<uint64_t>(keep, (uint64_t)s->opts.hbm_budget);
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
     s->loop_thread = std::thread([s] { s->loop_main(); });
     s->setup_thread = std::thread([s] { s->setup_main(); });
+    s->free_thread = std::thread([s] { s->free_main(); });
     *out = s;
     return SKG_OK;
 }
@@ -364,6 +407,12 @@ int skg_server_destroy(skg_server* s) {
     }
     s->setup_thread.join();
     s->loop_thread.join();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop_free = true;
+        s->free_cv.notify_all();
+    }
+    s->free_thread.join();                   // the retired contexts are freed
     {
         std::lock_guard<std::mutex> lk(s->mu);
         for (auto& kv : s->reqs) if (kv.second->ctx) { skg_ctx_destroy(kv.second->ctx); kv.second->ctx = nullptr; }

@@ -289,13 +289,15 @@ def _footprint(req, npix):
 
 def run_alone(req, device=0, npix=256, precision=A.PREC_FP32):
     """The plain single-simulation GPU path for one request: create, run one phase, read the frame.
-    Returns (frame, seconds)."""
+    Returns (frame, seconds until the frame is in host memory); the context is released after the
+    clock stops, as the served requests' latencies end when their frames are read."""
     t0 = time.perf_counter()
     ctx = runtime.Context(build_model(req, npix), device=device)
     ctx.run_phase(A.PHASE_STELLAR, [0, 1, 2], req.packets, 0, req.packets, seed=req.seed, precision=precision)
     cube, _ = ctx.read_instrument(0)
+    t = time.perf_counter() - t0
     ctx.close()
-    return cube[0], time.perf_counter() - t0
+    return cube[0], t
 
 
 def latency_stats(reqs):
