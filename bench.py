@@ -7,8 +7,9 @@ other configurations of the hot path with the same machinery:
   cartesian_oligo   oligochromatic disk on a 100x100x50 Cartesian grid, 300x300 frame + SED at 88 deg
   voronoi_clumpy    clumpy dust disk (10^4 clumps, 25 % of the mass) on a 10^6-site Voronoi grid
   kdtree_dust       panchromatic disk + point source on a k-d tree, 100 wavelengths 0.1-1000 micron,
-                    one step = stellar phase with absorption tallies + dust emission spectra +
-                    dust-emission phase
+                    one step = stellar phase with absorption tallies, two dust self-absorption
+                    cycles and the dust-emission phase (emission spectra recomputed before
+                    each dust phase)
 
 One step = the workload's phases (a sequence of waves: an event pass and a traversal pass each)
 over all wavelengths with --packets packets per wavelength per GPU (10^7 by default, the
@@ -65,6 +66,8 @@ def parse():
                    help="cache of the headline octree between runs of the same size (git-ignored)")
     p.add_argument("--serving", type=int, default=256,
                    help="requests of the fit-variant serving leg (Poisson 20/s; 0 = skip)")
+    p.add_argument("--serving-rates", type=lambda v: [float(x) for x in v.split(",") if x], default=[10.0],
+                   help="further arrival rates (per s) of the same requests, comma-separated ('' = none)")
     p.add_argument("--serving-impl", default="native", choices=["native", "python"],
                    help="the serving loop: the C ABI server (skg_submit/skg_poll) or the Python one")
     p.add_argument("--phase-only", action="store_true",
@@ -587,41 +590,62 @@ def _tally_len(ctx, i, sed=False):
 
 def serving_leg(args, device):
     """Fit-variant requests (oligochromatic disk, 3 wavelengths, Cartesian N^3 with N in 32..128,
-    packets per wavelength log-uniform in 1e5..1e7, one 256x256 frame) arriving as a Poisson stream
-    at 20/s, served by continuous batching; then every request alone on the idle device (the plain
-    single-simulation path), and the plain path serving the same stream one request at a time.
-    Latency = result in host memory minus arrival."""
+    packets per wavelength log-uniform in 1e5..1e7, one 256x256 frame) arriving as a Poisson stream,
+    served by continuous batching: at the configured 20/s, then the same requests at each rate of
+    --serving-rates; every request alone on the idle device (the plain single-simulation path); and
+    the plain path serving the stream one request at a time.  Latency = result in host memory minus
+    arrival."""
     import numpy as np
     from skirt7_b200 import serving
-    reqs = serving.fitskirt_requests(n=args.serving, rate=20.0, seed=2024)
-    t0 = time.perf_counter()
-    if args.serving_impl == "native":
-        done, nst = serving.serve_native(reqs, device=device, npix=256, max_slots=64)
-        ticks, tick_s, admit_s, peak = nst["ticks"], nst["tick_device_s"], None, None
-    else:
-        srv = serving.Server(device=device, max_slots=64, npix=256)
-        done = srv.serve(reqs, realtime=True)
-        srv.close()
-        ticks, tick_s, admit_s, peak = srv.ticks, srv.tick_gpu_s, srv.admit_s, srv.peak_resident
-    wall = time.perf_counter() - t0
+
+    def serve(rate):
+        reqs = serving.fitskirt_requests(n=args.serving, rate=rate, seed=2024)
+        t0 = time.perf_counter()
+        if args.serving_impl == "native":
+            done, nst = serving.serve_native(reqs, device=device, npix=256, max_slots=64)
+            ticks, tick_s, admit_s, peak = nst["ticks"], nst["tick_device_s"], None, None
+        else:
+            srv = serving.Server(device=device, max_slots=64, npix=256)
+            done = srv.serve(reqs, realtime=True)
+            srv.close()
+            ticks, tick_s, admit_s, peak = srv.ticks, srv.tick_gpu_s, srv.admit_s, srv.peak_resident
+        wall = time.perf_counter() - t0
+        return reqs, done, wall, ticks, tick_s, admit_s, peak
+
+    reqs, done, wall, ticks, tick_s, admit_s, peak = serve(20.0)
     st = serving.latency_stats(done)
+    # the same requests (the stream's parameters do not depend on the rate) alone on the idle device
     service = [serving.run_alone(r, device=device, npix=256)[1] for r in reqs]
     alone = sorted(service)
     a50, a99 = float(np.percentile(alone, 50)), float(np.percentile(alone, 99))
-    # the plain single-simulation path serving the same stream: one request at a time in arrival
-    # order, each taking its measured alone time (start = max(arrival, previous finish))
-    finish, plain = 0.0, []
-    for r, t in sorted(zip(reqs, service), key=lambda q: q[0].arrival):
-        finish = max(r.arrival, finish) + t
-        plain.append(finish - r.arrival)
-    f99 = float(np.percentile(plain, 99))
+
+    def plain_fifo(rq):
+        # the plain single-simulation path serving the stream: one request at a time in arrival
+        # order, each taking its measured alone time (start = max(arrival, previous finish))
+        finish, lat = 0.0, []
+        for r, t in sorted(zip(rq, service), key=lambda q: q[0].arrival):
+            finish = max(r.arrival, finish) + t
+            lat.append(finish - r.arrival)
+        return float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
+
+    f50, f99 = plain_fifo(reqs)
     packets = sum(3 * r.packets for r in reqs)
-    return {"impl": args.serving_impl, "requests": len(reqs), "arrival_rate_per_s": 20.0, "p50_s": st["p50_s"],
-            "p99_s": st["p99_s"], "alone_p50_s": a50, "alone_p99_s": a99, "p99_over_alone_p99": st["p99_s"] / a99,
-            "plain_fifo_p50_s": float(np.percentile(plain, 50)), "plain_fifo_p99_s": f99,
-            "p99_over_plain_fifo_p99": st["p99_s"] / f99,
-            "packets_per_s": packets / wall, "makespan_s": wall, "ticks": ticks,
-            "tick_device_s": tick_s, "admit_host_s": admit_s, "peak_resident": peak}
+    out = {"impl": args.serving_impl, "requests": len(reqs), "arrival_rate_per_s": 20.0, "p50_s": st["p50_s"],
+           "p99_s": st["p99_s"], "alone_p50_s": a50, "alone_p99_s": a99, "p99_over_alone_p99": st["p99_s"] / a99,
+           "plain_fifo_p50_s": f50, "plain_fifo_p99_s": f99, "p99_over_plain_fifo_p99": st["p99_s"] / f99,
+           "offered_packets_per_s": packets / max(r.arrival for r in reqs),
+           "packets_per_s": packets / wall, "device_packets_per_s": packets / tick_s if tick_s else None,
+           "makespan_s": wall, "ticks": ticks, "tick_device_s": tick_s, "admit_host_s": admit_s,
+           "peak_resident": peak, "other_rates": []}
+    for rate in args.serving_rates:
+        rq, dn, wl_s, tk, ts, _, _ = serve(rate)
+        s2 = serving.latency_stats(dn)
+        p50, p99 = plain_fifo(rq)
+        out["other_rates"].append({"arrival_rate_per_s": rate, "p50_s": s2["p50_s"], "p99_s": s2["p99_s"],
+                                   "p99_over_alone_p99": s2["p99_s"] / a99, "plain_fifo_p99_s": p99,
+                                   "offered_packets_per_s": packets / max(r.arrival for r in rq),
+                                   "makespan_s": wl_s, "ticks": tk, "tick_device_s": ts})
+    return out
 
 
 def cpu_baseline(args, wl, ctx):
