@@ -365,8 +365,9 @@ typedef struct skg_server skg_server;
 typedef struct skg_server_opts {
     int64_t hbm_budget;                     /* device bytes the admitted requests may hold together (0: 40 GiB) */
     int32_t max_slots;                      /* requests per launch, 1..64 (0: 64) */
-    int64_t tick_packets;                   /* packets per wavelength a request runs per tick at most (0: 2^22) */
-    int64_t tick_budget;                    /* packets (all wavelengths) one tick hands out (0: 48 * 2^20) */
+    int64_t tick_packets;                   /* packets per wavelength each ready request is given first in a tick
+                                               (0: 2^23); budget left after that goes to the oldest requests */
+    int64_t tick_budget;                    /* packets (all wavelengths) one tick hands out (0: 16 * 2^20) */
     int32_t precision;                      /* SKG_PREC_* of the traversal geometry */
 } skg_server_opts;
 typedef struct skg_request {

@@ -126,14 +126,6 @@ double grid_diag(const skg_grid& g) {
     return std::sqrt(dx * dx + dy * dy + dz * dz);
 }
 
-int64_t grid_ncells(const skg_grid& g) {
-    if (g.type == SKG_GRID_CARTESIAN) return (int64_t)g.nx * g.ny * g.nz;
-    if (g.type == SKG_GRID_VORONOI) return g.nsites;
-    int64_t c = 0;
-    for (int l = 0; l < g.nnodes; l++) if (g.node_cell[l] >= 0) c++;
-    return c;
-}
-
 // Uploads a grid into both precisions.
 DevGrid make_grid(Allocs& A, const skg_grid& g, cudaStream_t s) {
     DevGrid G;
@@ -822,7 +814,7 @@ int skg_run_phase(skg_ctx* ctx, int phase, const int32_t* ells, int nell, uint64
         int precision = opts ? opts->precision : SKG_PREC_FP32;
         int blocks = opts ? opts->blocks : 0;
         CK(cudaEventRecord(ctx->ev0, s));
-        CK(ctx->waves.begin(P, ctx->grid.type, tree_walk_of(ctx->grid), precision, 1, npool, blocks, s));
+        CK(ctx->waves.begin(P, ctx->grid.type, tree_walk_of(ctx->grid), precision, 1, npool, blocks, s, &g));
         CK(cudaEventRecord(ctx->ev1, s));
         return SKG_OK;
     } catch (const Failure& f) { return fail(ctx, f); }

@@ -165,6 +165,9 @@ struct WaveParams {
     int* freelist;                    // records the event pass freed (count: jcount[5])
     int* intlist;                     // records it found at their interaction point (jcount[6])
     float4* ckpt;                     // per packet record: checkpoints of its path walk
+    // the grid of a single-simulation launch: the traversal kernels' instantiation for one slot
+    // reads it from their parameters (constant-bank operands, no load instructions per cell step)
+    DevGrid g0;
 };
 
 // ---------------------------------------------------------------------------------------------

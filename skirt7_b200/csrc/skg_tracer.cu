@@ -33,6 +33,7 @@
 #include "skg_scene.cuh"
 #include "skg_internal.h"
 #include "skg_wave.h"
+#include <cstring>
 #include <type_traits>
 
 #include <chrono>
@@ -825,10 +826,16 @@ template<template<typename> class Stepper> struct TravBlocks<1, Stepper> { stati
 template<> struct TravBlocks<1, VoronoiStepper> { static constexpr int value = SKG_VOR_PATH_MIN_BLOCKS; };
 template<template<typename> class Stepper> struct TravBlocks<2, Stepper> { static constexpr int value = SKG_PEEL_MIN_BLOCKS; };
 
-template<typename R, template<typename> class Stepper, int MODE>
+template<typename R, template<typename> class Stepper, int MODE, bool ONE>
 __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_kernel(const WaveParams W) {
     extern __shared__ unsigned char smem_raw[];
     DevGrid* sg = reinterpret_cast<DevGrid*>(smem_raw);
+    // the grid of a job's slot: a single-simulation launch (ONE) reads it from the kernel's
+    // parameters, whose fields are constant-bank operands; a batch from the block's shared copy,
+    // which the compiler reloads after the shared-memory counter atomics of the loop
+    auto grid_of = [&](int sl) -> const DevGrid& {
+        if constexpr (ONE) return W.g0; else return sg[sl];
+    };
     __shared__ const DevScene* s_scene[MAX_SLOTS];
     __shared__ unsigned long long s_cnt[C_N];
     const RunParams& P = W.R;
@@ -876,7 +883,7 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
         const bool idle = (live & ~want & ~pend) == 0;      // no lane of the warp is walking
         if (pend && (__popc(pend) >= SKG_AFTER_LANES || idle)) {
             if (kind == 3) {
-                const DevGrid& g = sg[slot];
+                const DevGrid& g = grid_of(slot);
                 const DevScene& S = *s_scene[slot];
                 double L = W.pk[p].L, tau_int = 0;      // the packet's luminosity at the path start
                 const int rc = after_path(W, S, p, phase, ell, tau, v2, L, tau_int);
@@ -921,7 +928,7 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
                 R kx, ky, kz;
                 if (MODE != 2 && jb.y == JOB_MAIN) { kx = (R)K.kx; ky = (R)K.ky; kz = (R)K.kz; kind = 1; v1 = K.L; v2 = 0; nck = 0; }
                 else { kx = (R)S.gkx[jb.y]; ky = (R)S.gky[jb.y]; kz = (R)S.gkz[jb.y]; kind = 0; }
-                st.init(sg[slot], (R)K.x, (R)K.y, (R)K.z, kx, ky, kz, hint);
+                st.init(grid_of(slot), (R)K.x, (R)K.y, (R)K.z, kx, ky, kz, hint);
                 if (kind == 1 && hint == -2) W.pk[p].pos_cell = st.cell0;
                 tau = 0;
                 // entry segments outside the grid (m = -1) carry no optical depth: only the
@@ -931,7 +938,7 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
 
         if (j < 0 || kind == 3) continue;   // waiting for enough lanes to refill / end paths together
 
-        const DevGrid& g = sg[slot];
+        const DevGrid& g = grid_of(slot);
         const DevScene& S = *s_scene[slot];
         // one cell step of the job (m, ds, kappa*rho); true when it ended the job (a re-walk that
         // reached the interaction optical depth)
@@ -1219,20 +1226,20 @@ __global__ void __launch_bounds__(128) tail_kernel(const WaveParams W) {
 namespace {
 
 // Resident blocks of a traversal instantiation (persistent grid = this many blocks per SM x SMs).
-template<typename R, template<typename> class Stepper, int MODE>
+template<typename R, template<typename> class Stepper, int MODE, bool ONE>
 int resident_blocks(size_t smem) {
     static int per = 0, sms = 0;
     if (per == 0) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trav_kernel<R, Stepper, MODE>, 256, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trav_kernel<R, Stepper, MODE, ONE>, 256, smem);
         if (per <= 0) per = 1;
     }
     return sms * per;
 }
 
-template<typename R, template<typename> class Stepper>
+template<typename R, template<typename> class Stepper, bool ONE>
 cudaError_t enqueue_wave(const WaveParams& W, int nslots, int trav_blocks, cudaEvent_t mid, cudaStream_t s) {
     const size_t smem = (size_t)nslots * sizeof(DevGrid);
     event_kernel<R><<<(W.npool + SKG_EVENT_THREADS - 1) / SKG_EVENT_THREADS, SKG_EVENT_THREADS, 0, s>>>(W);
@@ -1255,10 +1262,10 @@ cudaError_t enqueue_wave(const WaveParams& W, int nslots, int trav_blocks, cudaE
     if (mid) cudaEventRecord(mid, s);
 #if SKG_SPLIT_TRAV
     // the path jobs, then the peel-off jobs in their lean kernel
-    trav_kernel<R, Stepper, 1><<<trav_blocks > 0 ? trav_blocks : resident_blocks<R, Stepper, 1>(smem), 256, smem, s>>>(W);
+    trav_kernel<R, Stepper, 1, ONE><<<trav_blocks > 0 ? trav_blocks : resident_blocks<R, Stepper, 1, ONE>(smem), 256, smem, s>>>(W);
 #if SKG_PDL
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(resident_blocks<R, Stepper, 2>(smem));
+    cfg.gridDim = dim3(resident_blocks<R, Stepper, 2, ONE>(smem));
     cfg.blockDim = dim3(256);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
@@ -1267,13 +1274,13 @@ cudaError_t enqueue_wave(const WaveParams& W, int nslots, int trav_blocks, cudaE
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, trav_kernel<R, Stepper, 2>, W);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, trav_kernel<R, Stepper, 2, ONE>, W);
     if (e != cudaSuccess) return e;
 #else
-    trav_kernel<R, Stepper, 2><<<resident_blocks<R, Stepper, 2>(smem), 256, smem, s>>>(W);
+    trav_kernel<R, Stepper, 2, ONE><<<resident_blocks<R, Stepper, 2, ONE>(smem), 256, smem, s>>>(W);
 #endif
 #else
-    trav_kernel<R, Stepper, 0><<<trav_blocks > 0 ? trav_blocks : resident_blocks<R, Stepper, 0>(smem), 256, smem, s>>>(W);
+    trav_kernel<R, Stepper, 0, ONE><<<trav_blocks > 0 ? trav_blocks : resident_blocks<R, Stepper, 0, ONE>(smem), 256, smem, s>>>(W);
 #endif
     return cudaGetLastError();
 }
@@ -1288,10 +1295,16 @@ using WaveFn = cudaError_t (*)(const WaveParams&, int, int, cudaEvent_t, cudaStr
 using TailFn = cudaError_t (*)(const WaveParams&, cudaStream_t);
 struct PassFns { WaveFn wave; TailFn tail; };
 
-template<typename R, template<typename> class Stepper>
-PassFns fns() { return {enqueue_wave<R, Stepper>, enqueue_tail<R, Stepper>}; }
+template<typename R, template<typename> class Stepper, bool ONE = false>
+PassFns fns() { return {enqueue_wave<R, Stepper, ONE>, enqueue_tail<R, Stepper>}; }
 
-PassFns pick(int grid_type, int tree_walk, int precision) {
+// the FP32 tree and Voronoi walks have a single-slot instantiation (the grid as a kernel parameter:
+// traversal pass of a phase, Voronoi disk 255 against 260 ms, k-d tree disk 1778 against 1800 ms,
+// octree disk 1443 against 1445 ms; the Cartesian walk, 64.5 against 64.1 ms, keeps its shared copy)
+template<template<typename> class Stepper>
+PassFns fns32(bool one) { return one ? fns<float, Stepper, true>() : fns<float, Stepper, false>(); }
+
+PassFns pick(int grid_type, int tree_walk, int precision, bool one) {
     const bool f64 = precision == SKG_PREC_FP64;
     switch (grid_type) {
     case SKG_GRID_CARTESIAN:
@@ -1300,10 +1313,10 @@ PassFns pick(int grid_type, int tree_walk, int precision) {
     case SKG_GRID_BINTREE:
         if (f64) return fns<double, TreeStepper>();
         if (tree_walk == TW_NODES) return fns<float, TreeNodeWalk>();
-        if (tree_walk == TW_LATTICE) return fns<float, TreeLatticeStepper>();
-        return fns<float, TreeStepper>();
+        if (tree_walk == TW_LATTICE) return fns32<TreeLatticeStepper>(one);
+        return fns32<TreeStepper>(one);
     default:
-        return f64 ? fns<double, VoronoiStepper>() : fns<float, VoronoiStepper>();
+        return f64 ? fns<double, VoronoiStepper>() : fns32<VoronoiStepper>(one);
     }
 }
 
@@ -1363,7 +1376,7 @@ cudaError_t WaveRunner::reserve(size_t pool, int ngroups, int grid_type) {
 }
 
 cudaError_t WaveRunner::enqueue(int n) {
-    WaveFn fn = pick(grid_type_, tree_walk_, precision_).wave;
+    WaveFn fn = pick(grid_type_, tree_walk_, precision_, one_).wave;
     cudaError_t e;
     for (int i = 0; i < n; i++) {
         const int w = waves_ + i, b = w & 1;
@@ -1373,6 +1386,7 @@ cudaError_t WaveRunner::enqueue(int n) {
         W.pjobs = jobs_[b ^ 1]; W.pjtau = jtau_[b ^ 1]; W.pjL = jL_[b ^ 1];
         W.last_busy = ctr_ + 16;
         W.freelist = free_; W.intlist = free_ + npool_; W.ckpt = ckpt_on_ ? ckpt_ : nullptr;
+        W.g0 = g0_;
         if ((e = cudaMemsetAsync(ctr_ + 8 * b, 0, 8 * sizeof(unsigned), stream_)) != cudaSuccess) return e;
         if (timed_) {
             while (ev_.size() < 3 * (size_t)(w + 1)) {
@@ -1395,9 +1409,11 @@ cudaError_t WaveRunner::enqueue(int n) {
 }
 
 cudaError_t WaveRunner::begin(const RunParams& P, int grid_type, int tree_walk, int precision, int nslots,
-                              size_t npool, int trav_blocks, cudaStream_t s) {
+                              size_t npool, int trav_blocks, cudaStream_t s, const DevGrid* one_grid) {
     if (npool == 0 || npool > cap_pool_) return cudaErrorInvalidValue;
     P_ = P; grid_type_ = grid_type; tree_walk_ = tree_walk; precision_ = precision; nslots_ = nslots;
+    one_ = one_grid != nullptr && nslots == 1;
+    if (one_) g0_ = *one_grid; else std::memset(&g0_, 0, sizeof(g0_));
     trav_blocks_ = trav_blocks; stream_ = s; npool_ = (int)npool; waves_ = 0; tail_ran_ = false;
     const char* td = std::getenv("SKG_TAIL_DIV");
     tail_div_ = td ? std::atoi(td) : tail_div;
@@ -1427,7 +1443,8 @@ cudaError_t WaveRunner::enqueue_tail() {
             if (!tail_ev_[i] && (e = cudaEventCreate(&tail_ev_[i])) != cudaSuccess) return e;
         if ((e = cudaEventRecord(tail_ev_[0], stream_)) != cudaSuccess) return e;
     }
-    if ((e = pick(grid_type_, tree_walk_, precision_).tail(W, stream_)) != cudaSuccess) return e;
+    W.g0 = g0_;
+    if ((e = pick(grid_type_, tree_walk_, precision_, one_).tail(W, stream_)) != cudaSuccess) return e;
     tail_ran_ = true;
     return timed_ ? cudaEventRecord(tail_ev_[1], stream_) : cudaSuccess;
 }

@@ -27,9 +27,10 @@ public:
     cudaError_t reserve(size_t pool, int ngroups, int grid_type);
     // Enqueues the reset of the pool and the first waves of a phase on stream s.  P holds the
     // staged tables; nslots the slots whose DevGrid the traversal pass keeps in shared memory;
-    // tree_walk the FP32 tree walk (TreeWalk) of tree grids.
+    // tree_walk the FP32 tree walk (TreeWalk) of tree grids; one_grid (host copy), when given with
+    // nslots = 1, the grid the FP32 traversal kernels take as a kernel parameter instead.
     cudaError_t begin(const RunParams& P, int grid_type, int tree_walk, int precision, int nslots,
-                      size_t npool, int trav_blocks, cudaStream_t s);
+                      size_t npool, int trav_blocks, cudaStream_t s, const DevGrid* one_grid = nullptr);
     // Waits for the enqueued waves and enqueues more until no packet is left; then records
     // `end` (if given) on the phase's stream.  timeout_ms < 0 waits without limit.
     cudaError_t finish(int timeout_ms, cudaEvent_t end, bool* timed_out);
@@ -71,6 +72,8 @@ private:
     cudaStream_t stream_ = nullptr;
     RunParams P_{};
     int grid_type_ = 0, precision_ = 0, nslots_ = 1, trav_blocks_ = 0;
+    bool one_ = false;                 // a single-slot launch with its grid in g0_
+    DevGrid g0_{};
     int tree_walk_ = TW_ROPE;
     int npool_ = 0;
     int waves_ = 0;
