@@ -167,6 +167,26 @@ SKG_D double step_kr(const DevScene& S, const St& st, float kext1, int m, int el
     }
 }
 
+// Optical depth of a cell step.  SKG_DTAU32: one dust component on an FP32 walk forms the step's
+// kappa*rho*ds in FP32 (the geometry's precision) before the FP64 sum (traversal pass of a phase,
+// octree disk 1387 against 1385 ms, k-d tree disk 1745 against 1744 ms: off).
+#ifndef SKG_DTAU32
+#define SKG_DTAU32 0
+#endif
+template<typename R, typename St>
+SKG_D double step_dtau(const DevScene& S, const St& st, float kext1, int m, int ell, R ds) {
+#if SKG_DTAU32
+    if constexpr (sizeof(R) == 4) {
+        if (kext1 >= 0.f) {
+            float r;
+            if constexpr (EmbeddedRho<St>::value) r = st.rho; else r = __ldg(S.rhof + m);
+            return (double)(kext1 * r * ds);
+        }
+    }
+#endif
+    return step_kr<R>(S, st, kext1, m, ell) * (double)ds;
+}
+
 // Instrument::detect for the members of one direction group after the shared traversal
 // (SEDInstrument.cpp:32-42, FrameInstrument.cpp:33-47, SimpleInstrument.cpp:35-49,
 // FullInstrument.cpp:109-177).  SED bins go to the block's private copy `psed` when it is given
@@ -940,11 +960,10 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
 
         const DevGrid& g = grid_of(slot);
         const DevScene& S = *s_scene[slot];
-        // one cell step of the job (m, ds, kappa*rho); true when it ended the job (a re-walk that
-        // reached the interaction optical depth)
-        auto take_step = [&](int m, R ds, double kr) -> bool {
+        // one cell step of the job (m, ds, its optical depth); true when it ended the job (a re-walk
+        // that reached the interaction optical depth)
+        auto take_step = [&](int m, R ds, double dtau) -> bool {
             c_steps++;
-            const double dtau = kr * (double)ds;
             if (kind == 0) {
                 tau += dtau;
             } else if (kind == 1) {
@@ -1001,7 +1020,7 @@ __global__ void __launch_bounds__(256, (TravBlocks<MODE, Stepper>::value)) trav_
             int m; R ds;
             if (st.walk(g, m, ds)) {
                 // one dust component: the FP32 tree walk carries the cell density in its leaf record
-                if (take_step(m, ds, step_kr<R>(S, st, kext1, m, ell))) break;
+                if (take_step(m, ds, step_dtau<R>(S, st, kext1, m, ell, ds))) break;
             } else {
                 at_edge();
                 break;
@@ -1043,8 +1062,7 @@ SKG_D double tail_tau(const DevGrid& g, const DevScene& S, int ell, R x, R y, R 
     int m; R ds;
     while (st.walk(g, m, ds)) {
         cnt[C_STEPS]++;
-        const double kr = step_kr<R>(S, st, kext1, m, ell);
-        tau += kr * (double)ds;
+        tau += step_dtau<R>(S, st, kext1, m, ell, ds);
     }
     cnt[C_TRAV]++; cnt[C_NBR] += st.nscanned(); cnt[C_FB] += st.fallbacks;
     if (st.steps > g.max_steps) { atomicOr(err, ERR_STEP_BUDGET); cnt[C_ERR]++; }
@@ -1090,8 +1108,7 @@ SKG_D void tail_path(const WaveParams& W, const DevGrid& g, const DevScene& S, i
     int m; R ds;
     while (st.walk(g, m, ds)) {
         cnt[C_STEPS]++;
-        const double kr = step_kr<R>(S, st, kext1, m, ell);
-        const double dtau = kr * (double)ds;
+        const double dtau = step_dtau<R>(S, st, kext1, m, ell, ds);
         cnt[C_ABS] += absorb_step<R>(S, phase, m, ell, dtau, v1, v2);
         tau += dtau;
         if constexpr (CKPT) {
@@ -1119,8 +1136,7 @@ SKG_D void tail_path(const WaveParams& W, const DevGrid& g, const DevScene& S, i
     }
     while (st.walk(g, m, ds)) {
         cnt[C_STEPS]++;
-        const double kr = step_kr<R>(S, st, kext1, m, ell);
-        const double tn = tau + kr * (double)ds, sn = s + (double)ds;
+        const double tn = tau + step_dtau<R>(S, st, kext1, m, ell, ds), sn = s + (double)ds;
         if (tn > tau_int) {
             K.s_int = s + ((tau_int - tau) / (tn - tau)) * (sn - s);
             K.int_cell = m;
