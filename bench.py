@@ -12,8 +12,8 @@ other configurations of the hot path with the same machinery:
                     each dust phase)
 
 One step = the workload's phases (a sequence of waves: an event pass and a traversal pass each)
-over all wavelengths with --packets packets per wavelength per GPU (10^7 by default, the
-configuration's count).  A step ends when its phases have finished (the host has seen the last
+over all wavelengths with --packets packets per wavelength per GPU (by default the
+configuration's count: 10^7, 10^8 for the Voronoi workload).  A step ends when its phases have finished (the host has seen the last
 wave's counters), so every step times exactly its own waves.  Ranks (one process per GPU; with
 --gpus N and no torchrun environment the script starts the N ranks itself) run disjoint packet
 ranges of one simulation and all-reduce the frames over NCCL at the end of each step (weak
@@ -50,7 +50,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="octree_pan", choices=WORKLOADS)
-    p.add_argument("--packets", type=float, default=1e7, help="packets per wavelength per GPU per step")
+    p.add_argument("--packets", type=float, default=None,
+                   help="packets per wavelength per GPU per step (default: the configuration's, 10^7; "
+                        "10^8 for voronoi_clumpy)")
     p.add_argument("--e2e-steps", type=int, default=5, help="steps of the end-to-end leg (at most --steps)")
     p.add_argument("--plain-packets", type=float, default=1e6,
                    help="packets per wavelength of the plain-GPU leg (one thread per packet; 0 = skip)")
@@ -74,7 +76,15 @@ def parse():
                    help="run one stellar phase of the workload (--packets per wavelength, the library's default "
                         "launch choices) and print its counters and pass times: the program the ncu captures "
                         "of a phase run")
-    return p.parse_args()
+    a = p.parse_args()
+    if a.packets is None:
+        a.packets = WORKLOAD_PACKETS[a.workload]
+    return a
+
+
+# packets per wavelength of a step: the configurations' counts (the Cartesian workload runs 10
+# times configuration 1's 10^6 so that the device is filled)
+WORKLOAD_PACKETS = {"octree_pan": 1e7, "cartesian_oligo": 1e7, "voronoi_clumpy": 1e8, "kdtree_dust": 1e7}
 
 
 def peaks():
@@ -224,7 +234,7 @@ class Workload:
     # (dram__bytes_read.sum + dram__bytes_write.sum over the traversal launches of a stellar phase
     # of this workload, divided by that phase's cell steps); roofline.traffic scales it by a
     # launch's cell steps, and says so.  Other workloads report no traffic.
-    NCU_DRAM_BYTES_PER_STEP = {"octree_pan": 11.40}
+    NCU_DRAM_BYTES_PER_STEP = {"octree_pan": 11.76}
 
     def frames(self):
         from skirt7_b200 import _abi as A

@@ -126,6 +126,12 @@ double grid_diag(const skg_grid& g) {
     return std::sqrt(dx * dx + dy * dy + dz * dz);
 }
 
+// the FP32 Cartesian walk computes the walls of evenly spaced grids (1) or loads them from the
+// plane tables for every grid (0)
+#ifndef SKG_CART_UNIFORM
+#define SKG_CART_UNIFORM 0
+#endif
+
 // Uploads a grid into both precisions.
 DevGrid make_grid(Allocs& A, const skg_grid& g, cudaStream_t s) {
     DevGrid G;
@@ -150,6 +156,17 @@ DevGrid make_grid(Allocs& A, const skg_grid& g, cudaStream_t s) {
         f.assign(g.yv, g.yv + g.ny + 1); G.yvf = upload(A, f.data(), f.size(), s);
         f.assign(g.zv, g.zv + g.nz + 1); G.zvf = upload(A, f.data(), f.size(), s);
         G.ncells = g.nx * g.ny * g.nz;
+        // evenly spaced planes (to 1e-9 of the spacing) on all three axes: the FP32 walk computes
+        // its walls
+        auto even = [](const double* v, int n, float& org, float& h) {
+            const double step = (v[n] - v[0]) / n;
+            for (int q = 0; q <= n; q++)
+                if (std::fabs(v[q] - (v[0] + q * step)) > 1e-9 * std::fabs(step)) return false;
+            org = (float)v[0]; h = (float)step;
+            return step > 0;
+        };
+        G.cart_uniform = SKG_CART_UNIFORM && even(g.xv, g.nx, G.corg[0], G.cstep[0]) &&
+                         even(g.yv, g.ny, G.corg[1], G.cstep[1]) && even(g.zv, g.nz, G.corg[2], G.cstep[2]);
     } else if (g.type == SKG_GRID_OCTREE || g.type == SKG_GRID_BINTREE) {
         int n = g.nnodes;
         REQUIRE(n > 0 && g.node_box && g.node_child && g.node_father && g.node_cell && g.node_dir, "tree grid needs node arrays");
@@ -1225,9 +1242,10 @@ int skg_batch_run(skg_batch* b, int phase, const skg_work* work, int nwork, cons
             auto tree = [](int t) { return t == SKG_GRID_OCTREE || t == SKG_GRID_BINTREE; };
             REQUIRE(w.ctx->grid.type == gtype || (tree(gtype) && tree(w.ctx->grid.type)),
                     "a batch holds one kind of grid");
-            const int bk = tree(gtype) ? tree_walk_of(w.ctx->grid) : TW_ROPE;
+            const int bk = tree_walk_of(w.ctx->grid);
             if (gbk < 0) gbk = bk;
-            REQUIRE(bk == gbk, "a batch holds trees of one walk kind (Bookkeeping search, rope or lattice records)");
+            if (gtype == SKG_GRID_CARTESIAN) gbk = std::min(gbk, bk);   // the plane tables serve every grid
+            else if (tree(gtype)) REQUIRE(bk == gbk, "a batch holds trees of one walk kind (Bookkeeping search, rope or lattice records)");
             if (phase != SKG_PHASE_STELLAR) REQUIRE(w.ctx->emit_cdf != nullptr, "dust phases need dust emission enabled");
             int slot = -1;
             for (int q = 0; q < nslots; q++) if (slots[q] == w.ctx) slot = q;

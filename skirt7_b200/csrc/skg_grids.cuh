@@ -28,6 +28,10 @@ struct DevGrid {
     int nx, ny, nz;
     const double *xv, *yv, *zv;
     const float  *xvf, *yvf, *zvf;
+    // evenly spaced planes on every axis (plane q at corg + q * cstep): the FP32 walk computes its
+    // walls instead of loading them
+    int cart_uniform;
+    float corg[3], cstep[3];
 
     // tree: node_box (6 doubles per node); nodef: 2 float4 per node
     //   nodef[2l]   = (xmin, ymin, zmin, int child0 or -1)
@@ -73,10 +77,13 @@ struct DevGrid {
     const double* vvol;        // Voronoi cell volumes
 };
 
-// The FP32 walk a tree grid takes: the node walk (Bookkeeping search), the 64-byte rope records or
-// their lattice form.
+// The FP32 walk a grid takes.  Trees: the node walk (Bookkeeping search), the 64-byte rope records
+// or their lattice form; Cartesian grids: the plane tables, or computed walls when every axis is
+// evenly spaced.
 enum TreeWalk : int { TW_ROPE = 0, TW_NODES = 1, TW_LATTICE = 2 };
+enum CartWalk : int { CW_TABLE = 0, CW_UNIFORM = 1 };
 inline int tree_walk_of(const DevGrid& g) {
+    if (g.type == SKG_GRID_CARTESIAN) return g.cart_uniform ? CW_UNIFORM : CW_TABLE;
     return g.search == SKG_SEARCH_BOOKKEEPING ? TW_NODES : g.lattice ? TW_LATTICE : TW_ROPE;
 }
 
@@ -401,6 +408,73 @@ struct CartStepper<float> : CartStepperRef<float> {
         return false;
     }
 #endif
+};
+
+// FP32 walk of a Cartesian grid whose planes are evenly spaced on every axis: the DDA of
+// CartStepper<float> with the ray parameter of plane q on axis a computed as t = c0_a + q dt_a
+// (c0 = (first plane - origin) / k, dt = spacing / k, fixed for a walk; one FMA) instead of loading
+// the plane and selecting its table, the origin and the reciprocal by axis.  The sign of dt is the
+// direction's, so the step needs no direction component either.
+template<typename R> struct CartUniStepper : CartStepperRef<R> {};
+template<>
+struct CartUniStepper<float> : CartStepperRef<float> {
+    float tx, ty, tz;           // ray parameter of the next x, y and z wall
+    float tc;                   // ray parameter of the current point
+    float cx, cy, cz;           // ray parameter of plane 0 per axis
+    float dtx, dty, dtz;        // per plane (0 for an axis with |k| <= 1e-15: never crossed)
+
+    SKG_D static void axis(float org, float h, float o, float k, int c, float& c0, float& dt, float& tn) {
+        if (fabsf(k) > 1e-15f) {
+            const float u = 1.f / k;
+            c0 = (org - o) * u; dt = h * u;
+            tn = fmaf((float)(k < 0.f ? c : c + 1), dt, c0);
+        } else {
+            c0 = 0.f; dt = 0.f; tn = FLT_MAX;
+        }
+    }
+    SKG_D void init(const DevGrid& g, float rx, float ry, float rz, float dx, float dy, float dz, int hint = -1) {
+        CartStepperRef<float>::init(g, rx, ry, rz, dx, dy, dz, hint);
+        tc = 0.f;
+        if (done) return;
+        if (isnan(kx) || isnan(ky) || isnan(kz)) { done = true; return; }   // the reference walk stops
+        axis(g.corg[0], g.cstep[0], x, kx, i, cx, dtx, tx);
+        axis(g.corg[1], g.cstep[1], y, ky, j, cy, dty, ty);
+        axis(g.corg[2], g.cstep[2], z, kz, k, cz, dtz, tz);
+    }
+    static constexpr bool resumable = false;
+    SKG_D bool next(const DevGrid& g, int& m, float& ds) {
+        if (pd.pop(ds)) { m = -1; return true; }
+        return walk(g, m, ds);
+    }
+    // one cell step: the crossed axis (the reference's tie order) and every per-axis value a select
+    SKG_D bool walk(const DevGrid& g, int& m, float& ds) {
+        while (!done) {
+            if (++steps > g.max_steps) { done = true; return false; }
+            m = k + g.nz * j + g.nz * g.ny * i;
+            const int a = (tx <= ty && tx <= tz) ? 0 : (ty <= tz ? 1 : 2);
+            const float t = a == 0 ? tx : (a == 1 ? ty : tz);
+            if (t != t) { done = true; return false; }   // NaN direction
+            const float dt = a == 0 ? dtx : (a == 1 ? dty : dtz);
+            const bool neg = dt < 0.f;
+            const int n = a == 0 ? g.nx : (a == 1 ? g.ny : g.nz);
+            const int q = (a == 0 ? i : (a == 1 ? j : k)) + (neg ? -1 : 1);
+            if (a == 0) i = q;
+            if (a == 1) j = q;
+            if (a == 2) k = q;
+            if (q >= n || q < 0) done = true;
+            else {
+                const float c0 = a == 0 ? cx : (a == 1 ? cy : cz);
+                const float tn = fmaf((float)(neg ? q : q + 1), dt, c0);
+                if (a == 0) tx = tn;
+                if (a == 1) ty = tn;
+                if (a == 2) tz = tn;
+            }
+            const float d = t - tc;
+            tc = t;
+            if (d > 0.f) { ds = d; return true; }   // DustGridPath::addSegment drops ds <= 0
+        }
+        return false;
+    }
 };
 
 // =============================================================================================

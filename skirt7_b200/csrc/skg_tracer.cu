@@ -1324,7 +1324,8 @@ PassFns pick(int grid_type, int tree_walk, int precision, bool one) {
     const bool f64 = precision == SKG_PREC_FP64;
     switch (grid_type) {
     case SKG_GRID_CARTESIAN:
-        return f64 ? fns<double, CartStepper>() : fns<float, CartStepper>();
+        if (f64) return fns<double, CartStepper>();
+        return tree_walk == CW_UNIFORM ? fns<float, CartUniStepper>() : fns<float, CartStepper>();
     case SKG_GRID_OCTREE:
     case SKG_GRID_BINTREE:
         if (f64) return fns<double, TreeStepper>();
