@@ -127,9 +127,10 @@ double grid_diag(const skg_grid& g) {
 }
 
 // the FP32 Cartesian walk computes the walls of evenly spaced grids (1) or loads them from the
-// plane tables for every grid (0)
+// plane tables for every grid (0): traversal pass of a 10^7-packet phase of the oligochromatic disk
+// 61.6 against 64.1 ms, a batch of 24 fit variants 571 against 605 ms
 #ifndef SKG_CART_UNIFORM
-#define SKG_CART_UNIFORM 0
+#define SKG_CART_UNIFORM 1
 #endif
 
 // Uploads a grid into both precisions.
