@@ -115,10 +115,13 @@ namespace skg {
 // cell steps a lane takes per pass of the traversal loop (the warp's refill and end-of-path votes
 // run once per pass): peel-off-job kernel, path-job kernel.  Traversal pass of a 10^7-packet
 // phase (octree disk / Cartesian disk): 1 and 1: 161 / 69.1 ms; 2 and 1: 156 / 68.6; 2 and 2: 153 /
-// 68.1; 2 and 3: 152.4 / 67.0; 2 and 4: 151.3 / 66.4; 3 or 4 steps in the peel-off kernel spill:
-// 165 / 68.3
+// 68.1; 2 and 3: 152.4 / 67.0; 2 and 4: 151.3 / 66.4; 3 or 4 steps in the peel-off kernel spilled
+// then: 165 / 68.3.  With the per-axis rope the peel-off kernel no longer spills at 3 or 4, and at
+// 2·10^6 packets per wavelength 3 and 4 take the octree disk 1360 ms against 1367 at 2 and 4 (4 and
+// 4: 1365, 2 and 6: 1404); 3 and 4 against 2 and 4 elsewhere: Cartesian disk 61.2 / 61.7, k-d tree
+// disk 1730 / 1734, Voronoi disk 252.8 / 253.4 ms, a batch of 24 fit variants 566 / 571 ms
 #ifndef SKG_INNER_STEPS
-#define SKG_INNER_STEPS 2
+#define SKG_INNER_STEPS 3
 #endif
 #ifndef SKG_INNER_PATH
 #define SKG_INNER_PATH 4
