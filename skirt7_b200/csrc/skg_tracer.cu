@@ -112,6 +112,15 @@ namespace skg {
 #ifndef SKG_LAUNCH_OCC
 #define SKG_LAUNCH_OCC 1
 #endif
+// the event pass's grid for pools of at most this many records: the blocks resident at once,
+// striding over the pool (the per-block counter and SED flushes then happen once per resident
+// block); larger pools: one thread per record.  Event pass of a 10^7-packet phase, pool 2^21:
+// Cartesian disk 15.7 against 16.8 ms, a batch of 24 fit variants 560.7 against 566.6 ms (whole
+// batch); pool 2^23 (2·10^6 packets per wavelength): octree disk 156 against 139 ms, k-d tree disk
+// 190 against 188 ms -- so the stride only up to 2^21
+#ifndef SKG_EVENT_STRIDE_POOL
+#define SKG_EVENT_STRIDE_POOL (1 << 21)
+#endif
 // cell steps a lane takes per pass of the traversal loop (the warp's refill and end-of-path votes
 // run once per pass): peel-off-job kernel, path-job kernel.  Traversal pass of a 10^7-packet
 // phase (octree disk / Cartesian disk): 1 and 1: 161 / 69.1 ms; 2 and 1: 156 / 68.6; 2 and 2: 153 /
@@ -563,7 +572,7 @@ SKG_D void append_jobs(const WaveParams& W, int p, Packet& K, int npeel, int nma
     if (nmain) W.jobs[bm + inm - 1] = make_int2(p, JOB_MAIN);
 }
 
-template<typename R>
+template<typename R, bool STRIDE>
 __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 / SKG_EVENT_THREADS) event_kernel(const WaveParams W) {
     __shared__ unsigned long long s_cnt[C_N];
     __shared__ double s_sed[SED_PRIV];
@@ -583,7 +592,11 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 
 #if SKG_LAUNCH_KERNEL
     const unsigned FULL = 0xffffffffu;
 #endif
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    // STRIDE: the resident blocks stride over the pool; otherwise one thread per record
+#pragma unroll 1
+    for (int base = blockIdx.x * blockDim.x, it = 0; STRIDE ? base < W.npool : it == 0;
+         base += gridDim.x * blockDim.x, it++) {
+    const int p = base + threadIdx.x;
 
     Packet K;
     int state = PK_DONE;
@@ -662,6 +675,7 @@ __global__ void __launch_bounds__(SKG_EVENT_THREADS, SKG_EVENT_MIN_BLOCKS * 256 
         W.pk[p] = K;
     }
 #endif
+    }   // records of this block
     __syncthreads();
     if (threadIdx.x < C_N && s_cnt[threadIdx.x]) atomicAdd(P.counters + threadIdx.x, s_cnt[threadIdx.x]);
     if (psed) {
@@ -1261,7 +1275,20 @@ int resident_blocks(size_t smem) {
 template<typename R, template<typename> class Stepper, bool ONE>
 cudaError_t enqueue_wave(const WaveParams& W, int nslots, int trav_blocks, cudaEvent_t mid, cudaStream_t s) {
     const size_t smem = (size_t)nslots * sizeof(DevGrid);
-    event_kernel<R><<<(W.npool + SKG_EVENT_THREADS - 1) / SKG_EVENT_THREADS, SKG_EVENT_THREADS, 0, s>>>(W);
+    const int need = (W.npool + SKG_EVENT_THREADS - 1) / SKG_EVENT_THREADS;
+    if (W.npool <= SKG_EVENT_STRIDE_POOL) {
+        static int esms = 0, eper = 1;
+        if (esms == 0) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&esms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&eper, event_kernel<R, true>, SKG_EVENT_THREADS, 0);
+            if (eper <= 0) eper = 1;
+        }
+        event_kernel<R, true><<<std::min(need, esms * eper), SKG_EVENT_THREADS, 0, s>>>(W);
+    } else {
+        event_kernel<R, false><<<need, SKG_EVENT_THREADS, 0, s>>>(W);
+    }
 #if SKG_LAUNCH_KERNEL
     {
         // a grid-stride pass: SKG_LAUNCH_OCC sizes it to the blocks that are resident at once
