@@ -112,7 +112,7 @@ namespace skg {
 #ifndef SKG_LAUNCH_OCC
 #define SKG_LAUNCH_OCC 1
 #endif
-// the event pass's grid for pools of at most this many records: the blocks resident at once,
+// the event pass's grid for pools of at most this many records of a Cartesian grid: the blocks resident at once,
 // striding over the pool (the per-block counter and SED flushes then happen once per resident
 // block); larger pools: one thread per record.  Event pass of a 10^7-packet phase, pool 2^21:
 // Cartesian disk 15.7 against 16.8 ms, a batch of 24 fit variants 560.7 against 566.6 ms (whole
@@ -1276,7 +1276,11 @@ template<typename R, template<typename> class Stepper, bool ONE>
 cudaError_t enqueue_wave(const WaveParams& W, int nslots, int trav_blocks, cudaEvent_t mid, cudaStream_t s) {
     const size_t smem = (size_t)nslots * sizeof(DevGrid);
     const int need = (W.npool + SKG_EVENT_THREADS - 1) / SKG_EVENT_THREADS;
-    if (W.npool <= SKG_EVENT_STRIDE_POOL) {
+    // (Cartesian grids only: the octree's event pass, detections into three 512^2 frames, is slower
+    // strided at any pool size -- 2^21: 52.2 against 44.8 ms over 150 launches -- its heavier
+    // records unevenly spread over the resident blocks)
+    constexpr bool cart = std::is_same<Stepper<R>, CartStepper<R>>::value || std::is_same<Stepper<R>, CartUniStepper<R>>::value;
+    if (cart && W.npool <= SKG_EVENT_STRIDE_POOL) {
         static int esms = 0, eper = 1;
         if (esms == 0) {
             int dev = 0;
