@@ -37,7 +37,7 @@ from skirt7_b200.scene import KPC, MICRON, TreeDustGrid, VoronoiDustGrid  # noqa
 EXT = (-20 * KPC, -20 * KPC, -2 * KPC, 20 * KPC, 20 * KPC, 2 * KPC)
 dp = C.POINTER(C.c_double)
 
-# the octree of the panchromatic disk
+# the octree of the panchromatic disk (configuration 2: max level 10, cell mass fraction 1e-6)
 OCTREE = dict(gtype=A.GRID_OCTREE, minLevel=2, maxLevel=10, maxMassFraction=1e-6, samples=100, seed=4357)
 OCTREE_ELLS = [8, 20, 36]            # 0.21, 0.65 and 2.9 micron of the 50-point grid
 # the k-d tree of the dust-emission disk (configuration 5)

@@ -10,7 +10,7 @@ deterministic scenes, tests/golden/scenes.py):
   * configuration 3's clumpy disk (tau_V 5, 10^4 clumps) on a 10^6-site Voronoi grid, a 300x300
     frame at 88 degrees.
 
-The tolerances are north_star's: every frame's 32x32-pixel blocks and every group of cells within
+The tolerances are the parity target's: every frame's 32x32-pixel blocks and every group of cells within
 3 sigma of the combined Monte Carlo noise (z of the batch means: at most 1 % of the elements plus
 two beyond 3 sigma, none beyond 5), and the total flux of every frame at every wavelength within
 0.3 % (the fixtures' standard errors are about 0.1 % or less, so 0.3 % is resolved), with
